@@ -1,0 +1,348 @@
+"""Benchmark: time steps per second of the forced 512^3 DNS (FFT grid 768^3) on B200.
+
+Workload (the forced-DNS configuration): N=512 retained modes per axis (3/2-rule
+FFT grid 768^3), seeded solenoidal field with E(k) ~ k^4 exp(-2 (k/4)^2) and
+u_rms=1, constant-power forcing eps=0.1 on shells K=1..2 (the reference's
+disabled forcing block src/HIT_LES.cpp:243-278 with eps_in=0.1), nu=4.90e-4
+(k_max*eta = 1.5 with k_max=N/2), self-adaptive time step (kappa scheme) with
+C_At=0.5, FP64 plain form.  A "step" is one HIT::New_Fractional_Step_Method.
+
+--gpus N runs N independent replicas (one box per GPU, one process per GPU);
+the solver has no data-path collective, so `value` is the sum over ranks
+(N*K steps / max over ranks of the device time) and scaling is weak.
+
+--impl reference times the reference algorithm on the host cores (the CPU
+oracle, a C restatement of the reference solver with OpenMP threads in its
+FFTs, as FFTW threads are in the reference) on a bounded sample of the same
+workload, and prints the same JSON line with "impl": "reference".
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_BOX = 512
+KP = 4.0
+EPS = 0.1
+C_AT = 0.5
+SEED = 2024
+METRIC = "time steps/s, forced DNS N=512 (FFT 768^3), FP64"
+
+
+def nu_for(N: int, eps: float = EPS) -> float:
+    """nu with k_max*eta = 1.5, eta=(nu^3/eps)^(1/4), k_max=N/2."""
+    kmax = N / 2
+    eta = 1.5 / kmax
+    return (eta ** 4 * eps) ** (1.0 / 3.0)
+
+
+def box_args(N: int, self_adaptive: bool = True):
+    from spns_b200.params import HitArgs
+    M = (3 * N) // 2
+    return HitArgs(Nx=N, Ny=N, Nz=N, Mx=M, My=M, Mz=M, nu=nu_for(N), C_Smag=0.0, C_At=C_AT, Lx=1, Ly=1, Lz=1,
+                   omega_x=0.0, omega_y=0.0, omega_z=0.0, Nx_file=-1, Ny_file=-1, Nz_file=-1, isReLambda=False,
+                   isInitialFieldFromBinaryFile=False, isInitialFieldFromASCIIFile=False, isNotCubic=False,
+                   isRotating=False, isLES=False, isComplexConjugateCorrected=False, isSelfAdaptive=self_adaptive)
+
+
+def algorithmic_bytes(N: int, self_adaptive: bool = True, word: int = 16):
+    """Bytes each kernel must move once (arrays read + written, each counted once)."""
+    h = N // 2
+    K, M, Kz = 2 * h + 1, (3 * N) // 2, h + 1
+    S0, S1, S2 = K * K * Kz, K * M * Kz, M * M * Kz
+    k5_state = (18 if self_adaptive else 12) * S0
+    return {
+        "k1_inv_x": (3 * S0 + 5 * S1) * word,
+        "k2_inv_y": (5 * S1 + 6 * S2) * word,
+        "k3_z": (6 * S2 + 3 * S2) * word,
+        "k4_fwd_y": (3 * S2 + 3 * S1) * word,
+        "k5_fwd_x_sweep": (3 * S1 + k5_state) * word,
+        "shell_sums": 3 * S0 * word,
+    }, dict(S0=S0, S1=S1, S2=S2)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"spns_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax = float(parts[2])
+                except ValueError:
+                    continue
+                for nm, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        sm.sort()
+        med = sm[len(sm) // 2] if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n_gpus: int):
+    if n_gpus <= 1 and "RANK" not in os.environ:
+        return 0, 1, 0, None
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    rank, world = int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", n_gpus))
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    torch.cuda.set_device(local)
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    return rank, world, local, dist
+
+
+def reduce_max(dist, value: float) -> float:
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# CPU oracle timing (reference arm and cpu_baseline)
+# ---------------------------------------------------------------------------
+def cpu_sample(n_sample: int, steps: int, threads: int):
+    """Times `steps` oracle steps of the same workload at N=n_sample; returns s/step."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from spns_b200.fields import seeded_spectral_field
+    a = box_args(n_sample)
+    a.nu = nu_for(N_BOX)
+    h = O.OracleHIT(a, k41_ranks=1, nthreads=threads, eps_forcing=EPS)
+    h.set_compact(seeded_spectral_field(n_sample, n_sample, n_sample, kp=KP, seed=SEED))
+    h.Recalculate_Velocity_Antitransform()
+    h.Recalculate_TimeStep()
+    h.New_Fractional_Step_Method()  # first step (untimed)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        h.New_Fractional_Step_Method()
+    return (time.perf_counter() - t0) / steps
+
+
+def fft_work(N: int) -> float:
+    M = (3 * N) // 2
+    return M ** 3 * math.log2(M ** 3)
+
+
+def cpu_baseline_block(threads: int, n_sample: int = 96, steps: int = 3):
+    s = cpu_sample(n_sample, steps, threads)
+    scale = fft_work(N_BOX) / fft_work(n_sample)
+    v = 1.0 / (s * scale)
+    return {"value": v, "unit": "steps/s", "cores": threads, "kind": "port",
+            "sample": (f"{steps} steps of the same forced DNS at N={n_sample} (FFT {(3 * n_sample) // 2}^3), "
+                       f"{s:.3f} s/step, extrapolated to N={N_BOX} by FFT work M^3 log2 M^3 (x{scale:.1f}); "
+                       f"the reference layout needs ~200 GB of host RAM at N={N_BOX}")}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", 0))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    n_sample = args.ref_sample_n
+    for _ in range(args.warmup):
+        cpu_sample(n_sample, 1, threads)
+    per = []
+    for _ in range(max(1, args.steps)):
+        per.append(cpu_sample(n_sample, 1, threads))
+    s = sum(per) / len(per)
+    scale = fft_work(N_BOX) / fft_work(n_sample)
+    value = 1.0 / (s * scale)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"forced DNS N={N_BOX} (FFT 768^3), eps=0.1 on K=1..2, self-adaptive dt",
+                   "sample": f"N={n_sample} per step, extrapolated"},
+        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": "port",
+                         "sample": f"one oracle step at N={n_sample} per timed step, {s:.3f} s, x{scale:.1f} FFT work to N={N_BOX}"},
+        "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_gpu(args):
+    import numpy as np
+    import torch
+    rank, world, local, dist = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    from spns_b200.hit import HIT
+    from spns_b200.fields import seeded_spectral_field
+
+    N = args.n
+    a = box_args(N)
+    h = HIT(a, device=local, eps_forcing=EPS)
+    U0 = seeded_spectral_field(N, N, N, kp=KP, seed=SEED + rank)
+    h.set_compact(U0)
+    del U0
+    h.Recalculate_Velocity_Antitransform()
+    h.Recalculate_TimeStep()
+    stream = torch.cuda.ExternalStream(h.stream_handle(), device=torch.device("cuda", local))
+
+    for _ in range(args.warmup):
+        h.New_Fractional_Step_Method()
+    nk = h.kernels_per_step()
+
+    # --- timed region: K steps on the solver's stream, per-kernel events inside ---
+    h.profile_begin(args.steps)
+    barrier(dist)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            h._ck(h._L.spns_step(h._h, 1))
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier(dist)
+    ms = ev0.elapsed_time(ev1)
+    names, per = h.profile_read(args.steps)
+    ms_max = reduce_max(dist, ms)
+
+    # --- e2e: the public API loop with a device->host read of the step's result ---
+    torch.cuda.synchronize()
+    barrier(dist)
+    nbins = h.getlast_rad_max() + 1
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        h.New_Fractional_Step_Method()
+        h.Recalculate_Energy_Cascade()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    e2e_max = reduce_max(dist, e2e_s)
+    s = h.scalars()
+    finite = math.isfinite(s.Ek_Tot) and math.isfinite(s.At)
+    h.close()
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+    value = world * args.steps / (ms_max / 1e3)
+    e2e_value = world * args.steps / e2e_max
+    # roofline of the dominant kernel
+    bytes_per, sizes = algorithmic_bytes(N)
+    mean_ms = per.mean(axis=0)
+    share = {n: float(m) for n, m in zip(names, mean_ms)}
+    dom = max((n for n in names if n in bytes_per), key=lambda n: share[n])
+    achieved = bytes_per[dom] / (share[dom] / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as fh:
+            traffic = json.load(fh).get(dom)
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: seeded solenoidal field, E(k)~k^4 exp(-2(k/4)^2), u_rms=1",
+        "config": {"workload": f"forced DNS N={N} (FFT {(3 * N) // 2}^3), eps=0.1 on K=1..2, nu={a.nu:.3e}, "
+                               "self-adaptive dt C_At=0.5, FP64 plain form",
+                   "N": N, "fft_grid": (3 * N) // 2, "parallelism": f"replicas x{world}",
+                   "l2": f"inputs larger than L2 (state {3 * sizes['S0'] * 16 / 1e9:.1f} GB, work buffers "
+                         f"{(5 * sizes['S1'] + 6 * sizes['S2']) * 16 / 1e9:.1f} GB)",
+                   "finite": finite},
+        "clocks": clk.summary(),
+        "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 8 * nbins + 8,
+                "loop": "HIT.New_Fractional_Step_Method() + Recalculate_Energy_Cascade() (E(K) to host) per step"},
+        "gpu_launches": nk * args.steps,
+        "kernel_ms": share,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+                     "algorithmic_bytes": bytes_per[dom]},
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_block(os.cpu_count() or 1)
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["spns", "reference"], default="spns")
+    ap.add_argument("--n", type=int, default=N_BOX, help="retained modes per axis (default 512)")
+    ap.add_argument("--ref-sample-n", type=int, default=96)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

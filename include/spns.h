@@ -1,0 +1,154 @@
+/*
+ * spns.h -- C ABI of libspns, the B200-native (sm_100a) pseudospectral time step.
+ *
+ * One handle = one periodic box solved the way the reference's class HIT
+ * (src/HIT_LES.h:21-246 of adalbal/SpNS) solves it, on one GPU, with no MPI.
+ * Each entry point replaces one HIT member (cited per function) so that a
+ * HIT_LES.cpp replacement can forward every call the reference driver
+ * (src/MAIN.cpp) makes.  Plain pointers and sizes only; host arrays belong to
+ * the caller and are copied; the handle owns every device buffer.
+ *
+ * Status codes: 0 = success, negative = error (see spns_status); the message of
+ * the last error of a handle is returned by spns_last_error().
+ */
+#ifndef SPNS_H
+#define SPNS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum spns_status {
+    SPNS_OK = 0,
+    SPNS_ERR_INVALID_ARGUMENT = -1,
+    SPNS_ERR_UNSUPPORTED_SIZE = -2, /* an FFT length outside the compiled set   */
+    SPNS_ERR_CUDA = -3,             /* a CUDA runtime call failed               */
+    SPNS_ERR_OUT_OF_MEMORY = -4,    /* device allocation refused                */
+    SPNS_ERR_NONFINITE = -5,        /* NaN/Inf met in the CFL maximum           */
+    SPNS_ERR_DOMAIN = -6            /* time-step angle outside [0, pi/2] (crash "Topt fail!") */
+} spns_status;
+
+typedef enum spns_precision {
+    SPNS_FP64 = 0,      /* plain form: every array and FFT in double            */
+    SPNS_FP32_HILO = 1  /* FFTs/products in float; spectral state as float hi/lo pair;
+                           reductions, CFL and forcing normalisation in double */
+} spns_precision;
+
+/* Arguments of the HIT constructor (src/HIT_LES.h:23-29), as src/MAIN.cpp:325
+ * passes them after its derivations (length-factor expansion of N and M,
+ * flags), plus options the reference does not have (marked "extension"). */
+typedef struct spns_hit_args {
+    int Nx, Ny, Nz;          /* retained modes per axis (expanded by length factors) */
+    int Mx, My, Mz;          /* 3/2-rule FFT grid per axis (expanded)                 */
+    double nu, C_Smag, C_At;
+    int Lx_factor, Ly_factor, Lz_factor;
+    double omega_x, omega_y, omega_z;
+    int Nx_file, Ny_file, Nz_file;
+    int isReLambda, isInitialFieldFromFile, isNotCubic, isRotating, isLES;
+    int isComplexConjugateCorrected, isSelfAdaptive;
+    /* extensions */
+    int precision;           /* spns_precision                                          */
+    int device;              /* CUDA device ordinal                                     */
+    int k41_ranks;           /* K41 initial field as generated by this many MPI ranks (>=1) */
+    double fixed_dt;         /* >0: constant time step instead of the CFL/self-adaptive one */
+    double eps_forcing;      /* >0: constant-power forcing on shells [eps_kmin, eps_kmax]   */
+    int eps_kmin, eps_kmax;  /*     (the disabled block src/HIT_LES.cpp:243-278, eps_in=eps) */
+    int nonlinear_form;      /* DNS only: 0 = advective u.grad(u) as the reference
+                                (src/HIT_LES.cpp:74-125, 12 inverse transforms), 1 = rotational
+                                omega x u (6 inverse transforms; equal to the advective form
+                                up to a gradient, hence identical after the projection only while
+                                the aliased +-N/2 modes of the 3/2 rule carry no energy) */
+} spns_hit_args;
+
+typedef struct spns_handle spns_handle;
+
+/* Scalars of the solver (getters of src/HIT_LES.h:187-201). */
+typedef struct spns_scalars {
+    double time, At, nu, Ek_Tot, Ok_Tot, ReLambda, Ek_init, Ek_init_file, Enstrophy_init_file;
+    double kappa, MaxVel;
+    int64_t iter, last_rad, last_rad_max;
+} spns_scalars;
+
+/* HIT::HIT + HIT_init (src/HIT_LES.h:23-84, src/HIT_LES.cpp:770-1092).
+ * file_uvw: initial physical velocity from the input file, three components one
+ * after another, each ActualNx_file*ActualNy_file*ActualNz_file doubles in
+ * [x][y][z] order (what src/HIT_LES.cpp:604-732 reads); NULL selects the K41
+ * initial field (src/HIT_LES.cpp:502-540). */
+int spns_create(const spns_hit_args *args, const double *file_uvw, spns_handle **out);
+/* HIT::~HIT (src/HIT_LES.h:86-88) */
+int spns_destroy(spns_handle *h);
+
+/* HIT::New_Fractional_Step_Method (src/HIT_LES.cpp:9-25), nsteps times. */
+int spns_step(spns_handle *h, int nsteps);
+/* HIT::Recalculate_TimeStep (src/HIT_LES.cpp:365-403) from the physical
+ * velocity of the last inverse transform. */
+int spns_recalculate_timestep(spns_handle *h);
+/* HIT::Forcing_Energy_Cascade (src/HIT_LES.cpp:410-444); Forced_Ek[0..last_input_rad]. */
+int spns_forcing_energy_cascade(spns_handle *h, const double *Forced_Ek, int last_input_rad, int nullify_missing);
+/* HIT::Forcing_Reynolds_Lambda (src/HIT_LES.cpp:485-489) */
+int spns_forcing_reynolds_lambda(spns_handle *h, double relambda);
+/* HIT::Recalculate_Reynolds_Lambda (src/HIT_LES.cpp:478-483) */
+int spns_recalculate_reynolds_lambda(spns_handle *h, double *relambda);
+/* HIT::Recalculate_Energy (src/HIT_LES.cpp:1254-1259) */
+int spns_recalculate_energy(spns_handle *h, double *ek_tot);
+/* HIT::Recalculate_Enstrophy (src/HIT_LES.cpp:490-495) */
+int spns_recalculate_enstrophy(spns_handle *h, double *ok_tot);
+/* HIT::Recalculate_Energy_Cascade (src/HIT_LES.cpp:1261-1266): Ek[0..last_rad_max]. */
+int spns_recalculate_energy_cascade(spns_handle *h, double *Ek, double *ek_tot);
+/* HIT::Recalculate_Velocity_Antitransform (src/HIT_LES.cpp:60-69): refreshes
+ * the physical velocity (and its CFL maximum) from the spectral state. */
+int spns_velocity_antitransform(spns_handle *h);
+/* HIT::Complex_Conjugate_Correction (src/HIT_LES.cpp:446-476) */
+int spns_complex_conjugate_correction(spns_handle *h);
+/* HIT::Check_PhysFour_Energy (src/HIT_LES.cpp:1216-1252): energies by the
+ * Fourier sum, the physical sum and the shell integral; *ok = all within atol. */
+int spns_check_physfour_energy(spns_handle *h, double atol, int *ok, double *diff1, double *diff2);
+
+/* getters / HIT::setnu (src/HIT_LES.h:187-201) */
+int spns_get_scalars(spns_handle *h, spns_scalars *out);
+int spns_set_nu(spns_handle *h, double nu);
+
+/* State access (HIT::FourierVelocity_to_BinaryFile / RealVelocity_to_BinaryFile
+ * data, src/HIT_LES_output.cpp:8-14).  Spectral layout: 3 components one after
+ * another, each [iy][ix][kz] with ix<Kx=2*(Nx'/2)+1, iy<Ky=2*(Ny'/2)+1,
+ * kz<=Nz'/2 (N' = retained modes before length-factor expansion), interleaved
+ * re/im doubles; ix maps to k1=ix (ix<=Nx'/2) or ix-Kx.  Physical layout: 3
+ * components, each [x][y][z] on the true FFT grid (ActualMx, ActualMy, ActualMz). */
+int spns_spectral_dims(spns_handle *h, int *Kx, int *Ky, int *Kz);
+int spns_physical_dims(spns_handle *h, int *Mx, int *My, int *Mz);
+int spns_get_spectral(spns_handle *h, double *uvw);
+int spns_set_spectral(spns_handle *h, const double *uvw);
+int spns_get_physical(spns_handle *h, double *uvw);
+
+/* Device-resident state for callers that keep their own device buffers:
+ * pointers to the three spectral components (layout as spns_get_spectral,
+ * element type double2 for SPNS_FP64). */
+int spns_device_state(spns_handle *h, void **u, void **v, void **w);
+/* The CUDA stream all work of the handle is issued on (cudaStream_t). */
+int spns_stream(spns_handle *h, void **stream);
+/* Number of kernels issued by the last spns_step call (per step). */
+int spns_kernels_per_step(spns_handle *h, int *count);
+
+/* Per-kernel CUDA-event profile of the next max_steps calls of one step
+ * (events recorded on the handle's stream between the kernels of a step). */
+int spns_profile_begin(spns_handle *h, int max_steps);
+/* ms[s*nkernels + k] = duration of kernel k in profiled step s (synchronises). */
+int spns_profile_read(spns_handle *h, float *ms, int cap, int *nkernels, int *nsteps);
+const char *spns_profile_kernel_name(spns_handle *h, int i);
+
+const char *spns_last_error(spns_handle *h);
+const char *spns_status_string(int status);
+
+/* Building block exposed for tests: batched 1-D complex FFT of `batch` contiguous
+ * length-n lines of device memory (double2), in place, unnormalised; sign=-1
+ * forward, +1 backward.  Replaces nothing in the reference (FFTW's 1-D plans,
+ * src/FFTW_package.cpp:47-56, are internal to its 3-D transforms). */
+int spns_fft1d_batch_f64(void *data_dev, int n, int batch, int sign);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPNS_H */

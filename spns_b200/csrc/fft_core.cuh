@@ -1,0 +1,186 @@
+// fft_core.cuh -- register/shared-memory Stockham FFT engine for sm_100a.
+//
+// One pencil of length L is processed by Q = L/E threads, each holding E
+// complex values in registers.  A stage of radix R performs E/R butterflies
+// per thread; between stages the values are exchanged through shared memory
+// (one buffer, two barriers per stage).  The first stage reads its inputs from
+// registers filled by the caller at rows  j + r*(L/R_first)  and the last stage
+// leaves its outputs in registers at rows  j + r*(L/R_last)  (j = q + Q*m), so
+// callers load pencils straight from global memory and store results straight
+// back (or keep them in registers for fused pointwise work).
+//
+// Stockham autosort, stage (R, Ns): butterfly j, k = j mod Ns,
+//   inputs  x_r = in[j + r*L/R],  x_r *= w_L^{r*k*L/(Ns*R)},  y = DFT_R(x),
+//   outputs out[(j/Ns)*Ns*R + k + r*Ns] = y_r.
+// Twiddles come from a table w_L^m = exp(-2*pi*i*m/L) computed on the host in
+// extended precision (the inverse uses the conjugate).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace spns {
+
+template <typename T> struct alignas(2 * sizeof(T)) cx { T x, y; };
+
+template <typename T> __device__ __forceinline__ cx<T> mk(T a, T b) { cx<T> r; r.x = a; r.y = b; return r; }
+template <typename T> __device__ __forceinline__ cx<T> operator+(cx<T> a, cx<T> b) { return mk<T>(a.x + b.x, a.y + b.y); }
+template <typename T> __device__ __forceinline__ cx<T> operator-(cx<T> a, cx<T> b) { return mk<T>(a.x - b.x, a.y - b.y); }
+template <typename T> __device__ __forceinline__ cx<T> operator*(T s, cx<T> a) { return mk<T>(s * a.x, s * a.y); }
+template <typename T> __device__ __forceinline__ cx<T> cmul(cx<T> a, cx<T> b) { return mk<T>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+template <typename T> __device__ __forceinline__ cx<T> cmulc(cx<T> a, cx<T> b) { return mk<T>(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y); }
+template <typename T> __device__ __forceinline__ cx<T> conj(cx<T> a) { return mk<T>(a.x, -a.y); }
+// i*a
+template <typename T> __device__ __forceinline__ cx<T> mul_i(cx<T> a) { return mk<T>(-a.y, a.x); }
+template <typename T> __device__ __forceinline__ cx<T> zero() { return mk<T>(T(0), T(0)); }
+
+// ---------------------------------------------------------------------------
+// Radix plan: greedy factors of L, each dividing E (8, 4, 2, then 3).
+// Forward order = greedy order, inverse order = reversed greedy order, so the
+// last radix of an inverse transform equals the first radix of a forward one
+// (register hand-off between them needs the same row mapping).
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int pick_radix(int rem, int E) {
+    return (rem % 8 == 0 && E % 8 == 0) ? 8
+         : (rem % 4 == 0 && E % 4 == 0) ? 4
+         : (rem % 2 == 0 && E % 2 == 0) ? 2
+         : (rem % 3 == 0 && E % 3 == 0) ? 3 : 0;
+}
+__host__ __device__ constexpr int n_stages(int L, int E) {
+    int n = 0, rem = L;
+    while (rem > 1) { int r = pick_radix(rem, E); if (r == 0) return -1; rem /= r; n++; }
+    return n;
+}
+__host__ __device__ constexpr int greedy_radix(int L, int E, int s) {
+    int rem = L;
+    for (int i = 0; i < s; i++) rem /= pick_radix(rem, E);
+    return pick_radix(rem, E);
+}
+template <int L, int E, bool INV> struct Plan {
+    static constexpr int NST = n_stages(L, E);
+    static_assert(NST > 0, "length not factorable with radices dividing E");
+    static_assert(L % E == 0, "E must divide L");
+    static constexpr int Q = L / E;
+    __host__ __device__ static constexpr int radix(int s) { return INV ? greedy_radix(L, E, NST - 1 - s) : greedy_radix(L, E, s); }
+    __host__ __device__ static constexpr int ns(int s) { int p = 1; for (int i = 0; i < s; i++) p *= radix(i); return p; }
+    static constexpr int R_first = radix(0);
+    static constexpr int R_last = radix(NST - 1);
+};
+
+// ---------------------------------------------------------------------------
+// Small DFTs (in place); INV selects exp(+2*pi*i/R).
+// ---------------------------------------------------------------------------
+template <typename T, bool INV> __device__ __forceinline__ void dft2(cx<T> *x) {
+    cx<T> a = x[0], b = x[1];
+    x[0] = a + b; x[1] = a - b;
+}
+template <typename T, bool INV> __device__ __forceinline__ void dft3(cx<T> *x) {
+    const T c3 = T(-0.5);
+    const T s3 = INV ? T(0.86602540378443864676372317075294) : T(-0.86602540378443864676372317075294);
+    cx<T> s = x[1] + x[2], d = x[1] - x[2];
+    cx<T> y0 = x[0] + s;
+    cx<T> m = mk<T>(x[0].x + c3 * s.x, x[0].y + c3 * s.y);
+    cx<T> e = mk<T>(-s3 * d.y, s3 * d.x);
+    x[0] = y0; x[1] = m + e; x[2] = m - e;
+}
+template <typename T, bool INV> __device__ __forceinline__ void dft4(cx<T> *x) {
+    cx<T> t0 = x[0] + x[2], t1 = x[0] - x[2], t2 = x[1] + x[3], t3 = x[1] - x[3];
+    cx<T> u = INV ? mk<T>(-t3.y, t3.x) : mk<T>(t3.y, -t3.x); // (+/-i)*t3
+    x[0] = t0 + t2; x[2] = t0 - t2; x[1] = t1 + u; x[3] = t1 - u;
+}
+template <typename T, bool INV> __device__ __forceinline__ void dft8(cx<T> *x) {
+    const T h = T(0.70710678118654752440084436210485);
+    cx<T> e[4] = {x[0], x[2], x[4], x[6]}, o[4] = {x[1], x[3], x[5], x[7]};
+    dft4<T, INV>(e); dft4<T, INV>(o);
+    // w8^k for k=1..3: forward exp(-i*pi*k/4)
+    cx<T> o1 = INV ? mk<T>(h * (o[1].x - o[1].y), h * (o[1].x + o[1].y)) : mk<T>(h * (o[1].x + o[1].y), h * (o[1].y - o[1].x));
+    cx<T> o2 = INV ? mk<T>(-o[2].y, o[2].x) : mk<T>(o[2].y, -o[2].x);
+    cx<T> o3 = INV ? mk<T>(-h * (o[3].x + o[3].y), h * (o[3].x - o[3].y)) : mk<T>(h * (o[3].y - o[3].x), -h * (o[3].x + o[3].y));
+    x[0] = e[0] + o[0]; x[4] = e[0] - o[0];
+    x[1] = e[1] + o1;   x[5] = e[1] - o1;
+    x[2] = e[2] + o2;   x[6] = e[2] - o2;
+    x[3] = e[3] + o3;   x[7] = e[3] - o3;
+}
+template <typename T, int R, bool INV> __device__ __forceinline__ void dft(cx<T> *x) {
+    if constexpr (R == 2) dft2<T, INV>(x);
+    else if constexpr (R == 3) dft3<T, INV>(x);
+    else if constexpr (R == 4) dft4<T, INV>(x);
+    else if constexpr (R == 8) dft8<T, INV>(x);
+}
+
+// ---------------------------------------------------------------------------
+// Stage engine.  SM is a shared-memory accessor:  cx<T>& SM::at(int row).
+// v[m*R + r] holds the input (before the stage) / output (after) of butterfly
+// j = q + Q*m, leg r.
+// ---------------------------------------------------------------------------
+template <typename T, int L, int E, bool INV, int S, class SM>
+__device__ __forceinline__ void fft_run(cx<T> (&v)[E], SM sm, int q, const cx<T> *__restrict__ tw) {
+    using PL = Plan<L, E, INV>;
+    constexpr int R = PL::radix(S);
+    constexpr int Ns = PL::ns(S);
+    constexpr int Q = PL::Q;
+    constexpr int MB = E / R;
+#pragma unroll
+    for (int m = 0; m < MB; m++) {
+        if constexpr (Ns > 1) {
+            const int j = q + Q * m;
+            const int k = j % Ns;
+#pragma unroll
+            for (int r = 1; r < R; r++) {
+                const cx<T> w = tw[r * k * (L / (Ns * R))];
+                v[m * R + r] = INV ? cmulc(v[m * R + r], w) : cmul(v[m * R + r], w);
+            }
+        }
+        dft<T, R, INV>(&v[m * R]);
+    }
+    if constexpr (S + 1 < PL::NST) {
+#pragma unroll
+        for (int m = 0; m < MB; m++) {
+            const int j = q + Q * m;
+            const int base = (j / Ns) * Ns * R + (j % Ns);
+#pragma unroll
+            for (int r = 0; r < R; r++) sm.at(base + r * Ns) = v[m * R + r];
+        }
+        __syncthreads();
+        constexpr int R2 = PL::radix(S + 1);
+        constexpr int MB2 = E / R2;
+#pragma unroll
+        for (int m = 0; m < MB2; m++) {
+            const int j = q + Q * m;
+#pragma unroll
+            for (int r = 0; r < R2; r++) v[m * R2 + r] = sm.at(j + r * (L / R2));
+        }
+        __syncthreads();
+        fft_run<T, L, E, INV, S + 1, SM>(v, sm, q, tw);
+    }
+}
+
+// Row of register slot e before the first stage (inputs) / after the last stage (outputs).
+template <int L, int E, bool INV> __device__ __forceinline__ int in_row(int q, int e) {
+    using PL = Plan<L, E, INV>;
+    constexpr int R = PL::R_first;
+    return q + PL::Q * (e / R) + (e % R) * (L / R);
+}
+template <int L, int E, bool INV> __device__ __forceinline__ int out_row(int q, int e) {
+    using PL = Plan<L, E, INV>;
+    constexpr int R = PL::R_last;
+    return q + PL::Q * (e / R) + (e % R) * (L / R);
+}
+
+template <typename T, int L, int E, bool INV, class SM>
+__device__ __forceinline__ void fft(cx<T> (&v)[E], SM sm, int q, const cx<T> *__restrict__ tw) {
+    fft_run<T, L, E, INV, 0, SM>(v, sm, q, tw);
+}
+
+// Accessor: tile of P pencils stored row-major [row][P] (pencil index fastest).
+template <typename T, int P> struct SmRowMajor {
+    cx<T> *base; int p;
+    __device__ __forceinline__ cx<T> &at(int row) const { return base[row * P + p]; }
+};
+// Accessor: pencil-major [p][L+pad], one padding slot every 8 rows.
+template <typename T, int L> struct SmPencil {
+    cx<T> *base;
+    static constexpr int PITCH = L + L / 8;
+    __device__ __forceinline__ cx<T> &at(int row) const { return base[row + (row >> 3)]; }
+};
+
+} // namespace spns

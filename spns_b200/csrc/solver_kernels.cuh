@@ -1,0 +1,837 @@
+// solver_kernels.cuh -- the five fused passes of one pseudospectral step and the
+// small kernels around them (B200 / sm_100a, bandwidth-bound, no tensor cores).
+//
+// Data layout in HBM (complex elements, kz contiguous everywhere):
+//   S0 compact spectral state   [iy][ix][kz]   Ky x Kx x Kz   (retained modes only)
+//   S1 after the x transform    [iy][x][kz]    Ky x Mx x Kz
+//   S2 after the y transform    [y][x][kz]     My x Mx x Kz
+// Kx=2*hx+1 (kx=-hx..hx), Ky=2*hy+1, Kz=hz+1 (kz=0..hz) with h=N/2: the 3/2-rule
+// box of the reference (src/HIT_LES.cpp:858-873, both +-N/2 kept for even N).
+// Wavenumbers are k = s*m with s the length factor of the axis, so a non-cubic
+// box of the reference (src/MAIN.cpp:216-260, src/HIT_LES.cpp:867-871) runs on
+// its true grid (ActualM) instead of the expanded one.
+//
+// Pass plan of one step (DNS, rotational form of the nonlinear term):
+//   K1 inverse x : S0 u,v,w          -> S1 u,v,w, w_y=i(kz u-kx w), i kx v
+//   K2 inverse y : S1 (5)            -> S2 u,v,w, w_x, w_y, w_z
+//   K3 z         : c2r of 6 fields, c = w x u (+ CFL maxima), r2c -> S2 c_x,c_y,c_z
+//   K4 forward y : S2 (3)            -> S1 (3)
+//   K5 forward x : S1 (3)            -> S0 spectral sweep: 1/M^3, R, Coriolis,
+//                  forcing, AB2 or kappa-scheme predictor, projection.
+// LES (Smagorinsky) carries the 9 velocity gradients and folds the divergence of
+// the SGS stress into the forward passes (i kz tau_i3 in K3, i ky tau_i2 in K4,
+// i kx tau_i1 in K5).
+#pragma once
+#include "fft_core.cuh"
+
+namespace spns {
+
+enum Mode { MODE_VEL = 0, MODE_ROT = 1, MODE_ADV = 2, MODE_LES = 3 };
+
+struct Geo {
+    int Kx, Ky, Kz;   // retained mode counts
+    int hx, hy, hz;   // half widths
+    int Mx, My, Mz;   // true FFT grid
+    int sx, sy, sz;   // wavenumber scale per axis (length factor)
+    long long S0, S1, S2; // elements per field in each layout
+};
+
+// Solver scalars living in device memory (read by kernels, updated by the
+// finisher), so that a captured step stays valid while they change.
+struct DevScalars {
+    double dt, time, nu, kappa, alpha;
+    double maxvel, phi0;
+    double ek_tot, ok_tot, relambda;
+    double sumsq_phys;                   // sum of u^2+v^2+w^2 over the grid (energy check)
+    unsigned long long max_bits[4];      // max|u|, max|v|, max|w|, max(|u|/Ax+|v|/Ay+|w|/Az)
+    long long iter;
+    int nonfinite, domain_err;
+};
+
+struct StepConsts {
+    double inv_norm;      // 1/(Mx*My*Mz) of the true grid
+    double omega_x, omega_y, omega_z;
+    double Ax, Ay, Az, inv_Ax, inv_Ay, inv_Az;
+    double C_At, Ah, t1;
+    double kopt_k[2], phi[3], c[14];
+    double les_ct;        // (C_Smag*delta)^2
+    double fixed_dt;
+    int eps_on, eps_kmin, eps_kmax;
+    int rotating, self_adaptive;
+};
+
+__device__ __forceinline__ int ffreq(int a, int M) { return a <= M / 2 ? a : a - M; }
+
+// Field counts of the work buffers per mode.
+template <int MODE> struct Fields {
+    static constexpr int K1 = MODE == MODE_VEL ? 3 : MODE == MODE_ROT ? 5 : 6;  // S1 after the inverse x pass
+    static constexpr int K2 = MODE == MODE_VEL ? 3 : MODE == MODE_ROT ? 6 : 9;  // S2 after the inverse y pass
+    static constexpr int K4 = MODE == MODE_LES ? 6 : 3;                         // S1 after the forward y pass
+};
+
+// ===========================================================================
+// K1: inverse transform along x.  Block = (kz chunk, iy).
+//   VEL: u,v,w   ROT: u,v,w, w_y=i(kz u-kx w), i kx v   ADV/LES: u,v,w, du/dx, dv/dx, dw/dx
+// ===========================================================================
+template <typename T, int L, int E, int P, int MODE>
+__global__ void __launch_bounds__(P *(L / E)) k1_inv_x(Geo g, const cx<T> *__restrict__ u, const cx<T> *__restrict__ v,
+                                                       const cx<T> *__restrict__ w, cx<T> *__restrict__ out,
+                                                       const cx<T> *__restrict__ tw) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int tid = threadIdx.x, p = tid % P, q = tid / P;
+    const int iy = blockIdx.y, kz = blockIdx.x * P + p;
+    const bool ok = kz < g.Kz;
+    const T kzf = T(g.sz * kz);
+    SmRowMajor<T, P> sm{reinterpret_cast<cx<T> *>(smraw), p};
+    const long long rb = (long long)iy * g.Kx;
+#pragma unroll 1
+    for (int f = 0; f < Fields<MODE>::K1; f++) {
+        cx<T> r[E];
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+            const int row = in_row<L, E, true>(q, e);
+            const int m1 = ffreq(row, L);
+            cx<T> val = zero<T>();
+            if (ok && m1 <= g.hx && m1 >= -g.hx) {
+                const long long idx = (rb + (m1 >= 0 ? m1 : m1 + g.Kx)) * g.Kz + kz;
+                const T kx = T(g.sx * m1);
+                if (f == 0) val = u[idx];
+                else if (f == 1) val = v[idx];
+                else if (f == 2) val = w[idx];
+                else if (MODE == MODE_ROT) {
+                    if (f == 3) { cx<T> a = u[idx], c = w[idx]; val = mul_i(mk<T>(kzf * a.x - kx * c.x, kzf * a.y - kx * c.y)); }
+                    else { val = mul_i(kx * v[idx]); }
+                } else { // x-derivatives
+                    const cx<T> *src = f == 3 ? u : f == 4 ? v : w;
+                    val = mul_i(kx * src[idx]);
+                }
+            }
+            r[e] = val;
+        }
+        fft<T, L, E, true>(r, sm, q, tw);
+        if (ok) {
+            cx<T> *o = out + (long long)f * g.S1 + (long long)iy * g.Mx * g.Kz + kz;
+#pragma unroll
+            for (int e = 0; e < E; e++) o[(long long)out_row<L, E, true>(q, e) * g.Kz] = r[e];
+        }
+    }
+}
+
+// ===========================================================================
+// K2: inverse transform along y.  Block = (kz chunk, x).
+//   ROT: u,v,w, w_x=i(ky w-kz v), w_y, w_z=i kx v - i ky u
+//   ADV/LES: u,v,w, du/dx,dv/dx,dw/dx, du/dy,dv/dy,dw/dy
+// ===========================================================================
+template <typename T, int L, int E, int P, int MODE>
+__global__ void __launch_bounds__(P *(L / E)) k2_inv_y(Geo g, const cx<T> *__restrict__ in, cx<T> *__restrict__ out,
+                                                       const cx<T> *__restrict__ tw) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int tid = threadIdx.x, p = tid % P, q = tid / P;
+    const int x = blockIdx.y, kz = blockIdx.x * P + p;
+    const bool ok = kz < g.Kz;
+    const T kzf = T(g.sz * kz);
+    SmRowMajor<T, P> sm{reinterpret_cast<cx<T> *>(smraw), p};
+    const long long col = (long long)x * g.Kz + kz;
+#pragma unroll 1
+    for (int f = 0; f < Fields<MODE>::K2; f++) {
+        cx<T> r[E];
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+            const int row = in_row<L, E, true>(q, e);
+            const int m2 = ffreq(row, L);
+            cx<T> val = zero<T>();
+            if (ok && m2 <= g.hy && m2 >= -g.hy) {
+                const cx<T> *F = in + (long long)(m2 >= 0 ? m2 : m2 + g.Ky) * g.Mx * g.Kz + col;
+                const T ky = T(g.sy * m2);
+                if (MODE == MODE_VEL) {
+                    val = F[(long long)f * g.S1];
+                } else if (MODE == MODE_ROT) {
+                    if (f < 3) val = F[(long long)f * g.S1];
+                    else if (f == 3) { cx<T> vv = F[g.S1], ww = F[2 * g.S1]; val = mul_i(mk<T>(ky * ww.x - kzf * vv.x, ky * ww.y - kzf * vv.y)); }
+                    else if (f == 4) val = F[3 * g.S1];
+                    else { cx<T> a = F[4 * g.S1], uu = F[0]; val = a - mul_i(ky * uu); }
+                } else {
+                    if (f < 6) val = F[(long long)f * g.S1];
+                    else val = mul_i(ky * F[(long long)(f - 6) * g.S1]);
+                }
+            }
+            r[e] = val;
+        }
+        fft<T, L, E, true>(r, sm, q, tw);
+        if (ok) {
+            cx<T> *o = out + (long long)f * g.S2 + col;
+#pragma unroll
+            for (int e = 0; e < E; e++) o[(long long)out_row<L, E, true>(q, e) * g.Mx * g.Kz] = r[e];
+        }
+    }
+}
+
+// ===========================================================================
+// K3: along z.  c2r of two real fields per complex transform (a + i b with
+// Hermitian extension; the kz=0 entries keep their real parts only, as a c2r of
+// the reference does), pointwise products on the grid, r2c of the products
+// (again two per transform) truncated to kz<=hz.  Block = P consecutive
+// pencils; each thread keeps the values of its own grid rows in registers, so
+// the inverse/forward hand-off needs no shared-memory round trip.
+// ===========================================================================
+// Loads the 2-for-1 spectrum Z = Xa + i Xb at the thread's input rows.
+// ma/mb: multiply the field by i*kz (z derivative) first.
+template <typename T, int L, int E>
+__device__ __forceinline__ void k3_load_pair(cx<T> (&r)[E], const cx<T> *__restrict__ A, bool ma, const cx<T> *__restrict__ B,
+                                             bool mb, int Kz, T sz, int q, bool ok) {
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+        const int row = in_row<L, E, true>(q, e);
+        cx<T> z = zero<T>();
+        if (ok) {
+            const bool lo = row < Kz, hi = row > L - Kz;
+            if (lo || hi) {
+                const int kk = lo ? row : L - row;
+                cx<T> a = A[kk], b = B ? B[kk] : zero<T>();
+                if (ma) a = mul_i(T(kk) * sz * a);
+                if (mb) b = mul_i(T(kk) * sz * b);
+                if (row == 0) z = mk<T>(a.x, b.x);
+                else if (lo) z = mk<T>(a.x - b.y, a.y + b.x);
+                else z = mk<T>(a.x + b.y, b.x - a.y);
+            }
+        }
+        r[e] = z;
+    }
+}
+
+template <typename T> __device__ __forceinline__ void block_max4(const double (&v)[4], DevScalars *ds) {
+    __shared__ double red[4][32];
+    double m[4] = {v[0], v[1], v[2], v[3]};
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int i = 0; i < 4; i++) m[i] = fmax(m[i], __shfl_xor_sync(0xffffffffu, m[i], o));
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    if (lane == 0)
+#pragma unroll
+        for (int i = 0; i < 4; i++) red[i][wid] = m[i];
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) m[i] = lane < nw ? red[i][lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+            for (int i = 0; i < 4; i++) m[i] = fmax(m[i], __shfl_xor_sync(0xffffffffu, m[i], o));
+        if (lane == 0)
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                double x = m[i];
+                if (!(x <= 1.7976931348623157e308)) atomicExch(&ds->nonfinite, 1); // NaN or Inf
+                else atomicMax(&ds->max_bits[i], (unsigned long long)__double_as_longlong(x));
+            }
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void block_sum(double v, double *dst) {
+    __shared__ double red[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        v = lane < nw ? red[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) atomicAdd(dst, v);
+    }
+    __syncthreads();
+}
+
+// Forward transform of the register pair z = a + i b and extraction of both
+// half spectra for kz < Kz:  Xa = (Z_k + conj Z_{L-k})/2, Xb = (Z_k - conj Z_{L-k})/(2i).
+// With jz: Xa += i kz Xb (the z-derivative of b folded into a; SGS divergence).
+template <typename T, int L, int E>
+__device__ __forceinline__ void k3_store_pair(cx<T> (&r)[E], SmPencil<T, L> sm, int q, int Kz, cx<T> *A, cx<T> *B,
+                                              bool fold_dz_b_into_a, T sz, bool ok, const cx<T> *__restrict__ tw) {
+    constexpr int Q = L / E;
+    fft<T, L, E, false>(r, sm, q, tw);
+#pragma unroll
+    for (int e = 0; e < E; e++) sm.at(out_row<L, E, false>(q, e)) = r[e];
+    __syncthreads();
+    if (ok) {
+        const T h = T(0.5);
+        for (int k = q; k < Kz; k += Q) {
+            cx<T> zk = sm.at(k), zm = sm.at(k == 0 ? 0 : L - k);
+            cx<T> xa = mk<T>(h * (zk.x + zm.x), h * (zk.y - zm.y));
+            cx<T> xb = mk<T>(h * (zk.y + zm.y), h * (zm.x - zk.x));
+            if (fold_dz_b_into_a) xa = xa + mul_i(T(k) * sz * xb);
+            A[k] = xa;
+            if (B) B[k] = xb;
+        }
+    }
+    __syncthreads();
+}
+
+// Single real field: forward transform of (a + 0i), kz < Kz written directly.
+template <typename T, int L, int E>
+__device__ __forceinline__ void k3_store_single(cx<T> (&r)[E], SmPencil<T, L> sm, int q, int Kz, cx<T> *A, bool ok,
+                                                const cx<T> *__restrict__ tw) {
+    fft<T, L, E, false>(r, sm, q, tw);
+    if (ok) {
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+            const int row = out_row<L, E, false>(q, e);
+            if (row < Kz) A[row] = r[e];
+        }
+    }
+}
+
+// Running CFL maxima; a NaN or Inf velocity turns the maxima into +Inf (fmax
+// alone would drop NaN), which the block reduction reports as non-finite.
+template <typename T>
+__device__ __forceinline__ void cfl_update(double (&mx)[4], double uu, double vv, double ww, const StepConsts &c) {
+    const double au = fabs(uu), av = fabs(vv), aw = fabs(ww);
+    const double s = au * c.inv_Ax + av * c.inv_Ay + aw * c.inv_Az;
+    if (!(s <= 1.7976931348623157e308)) { mx[0] = mx[1] = mx[2] = mx[3] = __longlong_as_double(0x7ff0000000000000LL); return; }
+    mx[0] = fmax(mx[0], au); mx[1] = fmax(mx[1], av); mx[2] = fmax(mx[2], aw);
+    mx[3] = fmax(mx[3], s);
+}
+
+// Shared-memory slots of physical fields kept per pencil (rows of this thread only).
+template <int MODE> struct K3Phys { static constexpr int N = MODE == MODE_ADV ? 3 : MODE == MODE_LES ? 9 : 0; };
+
+template <typename T, int L, int E, int P, int MODE>
+__global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ buf, StepConsts c, DevScalars *ds,
+                                                   double *__restrict__ phys, const cx<T> *__restrict__ tw) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    constexpr int Q = L / E;
+    constexpr int NPH = K3Phys<MODE>::N;
+    const int tid = threadIdx.x, p = tid / Q, q = tid % Q;
+    const long long npen = (long long)g.Mx * g.My;
+    const long long pen = (long long)blockIdx.x * P + p;
+    const bool ok = pen < npen;
+    const long long base = (ok ? pen : 0) * g.Kz;
+    cx<T> *smc = reinterpret_cast<cx<T> *>(smraw);
+    SmPencil<T, L> sm{smc + p * SmPencil<T, L>::PITCH};
+    T *ph = reinterpret_cast<T *>(smc + P * SmPencil<T, L>::PITCH) + (long long)p * NPH * L;
+    const T sz = T(g.sz);
+    cx<T> *F[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) F[i] = buf + (long long)i * g.S2 + base;
+    double mx[4] = {0.0, 0.0, 0.0, 0.0};
+
+    if constexpr (MODE == MODE_VEL) {
+        cx<T> A[E], B[E];
+        k3_load_pair<T, L, E>(A, F[0], false, F[1], false, g.Kz, sz, q, ok);
+        fft<T, L, E, true>(A, sm, q, tw);
+        k3_load_pair<T, L, E>(B, F[2], false, nullptr, false, g.Kz, sz, q, ok);
+        fft<T, L, E, true>(B, sm, q, tw);
+        double ss = 0.0;
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+            const double uu = A[e].x, vv = A[e].y, ww = B[e].x;
+            cfl_update<T>(mx, uu, vv, ww, c);
+            ss += uu * uu + vv * vv + ww * ww;
+        }
+        if (!ok) { mx[0] = mx[1] = mx[2] = mx[3] = 0.0; ss = 0.0; }
+        if (phys && ok) {
+            const int y = (int)(pen / g.Mx), x = (int)(pen % g.Mx);
+            const long long n3 = (long long)g.Mx * g.My * g.Mz;
+            double *o = phys + ((long long)x * g.My + y) * g.Mz;
+#pragma unroll
+            for (int e = 0; e < E; e++) {
+                const int row = out_row<L, E, true>(q, e);
+                o[row] = A[e].x; o[n3 + row] = A[e].y; o[2 * n3 + row] = B[e].x;
+            }
+        }
+        block_max4<T>(mx, ds);
+        block_sum(ss, &ds->sumsq_phys);
+    } else if constexpr (MODE == MODE_ROT) {
+        // pairs (u, w_x), (v, w_y), (w, w_z);  c = w x u  (= u.grad u + gradient)
+        cx<T> A[E], B[E], C[E];
+        k3_load_pair<T, L, E>(A, F[0], false, F[3], false, g.Kz, sz, q, ok);
+        fft<T, L, E, true>(A, sm, q, tw);
+        k3_load_pair<T, L, E>(B, F[1], false, F[4], false, g.Kz, sz, q, ok);
+        fft<T, L, E, true>(B, sm, q, tw);
+        k3_load_pair<T, L, E>(C, F[2], false, F[5], false, g.Kz, sz, q, ok);
+        fft<T, L, E, true>(C, sm, q, tw);
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+            const T uu = A[e].x, ox = A[e].y, vv = B[e].x, oy = B[e].y, ww = C[e].x, oz = C[e].y;
+            cfl_update<T>(mx, uu, vv, ww, c);
+            A[e] = mk<T>(oy * ww - oz * vv, oz * uu - ox * ww);
+            B[e] = mk<T>(ox * vv - oy * uu, T(0));
+        }
+        if (!ok) { mx[0] = mx[1] = mx[2] = mx[3] = 0.0; }
+        block_max4<T>(mx, ds);
+        k3_store_pair<T, L, E>(A, sm, q, g.Kz, F[0], F[1], false, sz, ok, tw);
+        k3_store_single<T, L, E>(B, sm, q, g.Kz, F[2], ok, tw);
+    } else {
+        // Advective form of the reference (src/HIT_LES.cpp:74-125): conv_i = u_j d_j u_i.
+        // S2 inputs: 0 u, 1 v, 2 w, 3 du/dx, 4 dv/dx, 5 dw/dx, 6 du/dy, 7 dv/dy, 8 dw/dy;
+        // z-derivatives are formed here from u, v, w.
+        // LES (src/HIT_LES.cpp:130-171): strain combinations a_ij accumulate in shared memory.
+        T cxv[E], cyv[E], czv[E];
+        cx<T> A[E];
+        auto PH = [&](int slot, int row) -> T & { return ph[slot * L + row]; };
+        // (u, v)
+        k3_load_pair<T, L, E>(A, F[0], false, F[1], false, g.Kz, sz, q, ok);
+        fft<T, L, E, true>(A, sm, q, tw);
+#pragma unroll
+        for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); PH(0, row) = A[e].x; PH(1, row) = A[e].y; }
+        // (w, du/dz)
+        k3_load_pair<T, L, E>(A, F[2], false, F[0], true, g.Kz, sz, q, ok);
+        fft<T, L, E, true>(A, sm, q, tw);
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+            const int row = out_row<L, E, true>(q, e);
+            const T ww = A[e].x;
+            PH(2, row) = ww;
+            cfl_update<T>(mx, PH(0, row), PH(1, row), ww, c);
+            cxv[e] = ww * A[e].y;
+            if (MODE == MODE_LES) PH(6, row) = A[e].y; // a13 = du/dz (+ dw/dx below)
+        }
+        // (du/dx, du/dy)
+        k3_load_pair<T, L, E>(A, F[3], false, F[6], false, g.Kz, sz, q, ok);
+        fft<T, L, E, true>(A, sm, q, tw);
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+            const int row = out_row<L, E, true>(q, e);
+            cxv[e] = PH(0, row) * A[e].x + PH(1, row) * A[e].y + cxv[e];
+            if (MODE == MODE_LES) { PH(3, row) = A[e].x; PH(4, row) = A[e].y; } // a11, a12 (partial)
+        }
+        // (dv/dx, dv/dy)
+        k3_load_pair<T, L, E>(A, F[4], false, F[7], false, g.Kz, sz, q, ok);
+        fft<T, L, E, true>(A, sm, q, tw);
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+            const int row = out_row<L, E, true>(q, e);
+            cyv[e] = PH(0, row) * A[e].x + PH(1, row) * A[e].y;
+            if (MODE == MODE_LES) { PH(4, row) = PH(4, row) + A[e].x; PH(5, row) = A[e].y; } // a12, a22
+        }
+        // (dw/dx, dw/dy)
+        k3_load_pair<T, L, E>(A, F[5], false, F[8], false, g.Kz, sz, q, ok);
+        fft<T, L, E, true>(A, sm, q, tw);
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+            const int row = out_row<L, E, true>(q, e);
+            czv[e] = PH(0, row) * A[e].x + PH(1, row) * A[e].y;
+            if (MODE == MODE_LES) { PH(6, row) = PH(6, row) + A[e].x; PH(7, row) = A[e].y; } // a13, a23 (partial)
+        }
+        // (dv/dz, dw/dz)
+        k3_load_pair<T, L, E>(A, F[1], true, F[2], true, g.Kz, sz, q, ok);
+        fft<T, L, E, true>(A, sm, q, tw);
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+            const int row = out_row<L, E, true>(q, e);
+            const T ww = PH(2, row);
+            cyv[e] = cyv[e] + ww * A[e].x;
+            czv[e] = czv[e] + ww * A[e].y;
+            if (MODE == MODE_LES) { PH(7, row) = PH(7, row) + A[e].x; PH(8, row) = A[e].y; } // a23, a33
+        }
+        if (!ok) { mx[0] = mx[1] = mx[2] = mx[3] = 0.0; }
+        block_max4<T>(mx, ds);
+        if constexpr (MODE == MODE_ADV) {
+#pragma unroll
+            for (int e = 0; e < E; e++) A[e] = mk<T>(cxv[e], cyv[e]);
+            k3_store_pair<T, L, E>(A, sm, q, g.Kz, F[0], F[1], false, sz, ok, tw);
+#pragma unroll
+            for (int e = 0; e < E; e++) A[e] = mk<T>(czv[e], T(0));
+            k3_store_single<T, L, E>(A, sm, q, g.Kz, F[2], ok, tw);
+        } else {
+            // eddy viscosity and SGS stress (src/HIT_LES.cpp:130-154), kept in the a_ij slots:
+            // slot 3 t11, 4 t12, 5 t22, 6 t13, 7 t23, 8 t33
+            const T ct = T(c.les_ct);
+#pragma unroll
+            for (int e = 0; e < E; e++) {
+                const int row = out_row<L, E, true>(q, e);
+                const T a11 = PH(3, row), a12 = PH(4, row), a22 = PH(5, row), a13 = PH(6, row), a23 = PH(7, row), a33 = PH(8, row);
+                T ne = T(2.0) * a11 * a11;
+                ne += T(2.0) * a22 * a22;
+                ne += T(2.0) * a33 * a33;
+                ne += a12 * a12;
+                ne += a13 * a13;
+                ne += a23 * a23;
+                ne = ct * sqrt(ne);
+                PH(3, row) = T(-2.0) * ne * a11;
+                PH(4, row) = T(-1.0) * ne * a12;
+                PH(5, row) = T(-2.0) * ne * a22;
+                PH(6, row) = T(-1.0) * ne * a13;
+                PH(7, row) = T(-1.0) * ne * a23;
+                PH(8, row) = T(-2.0) * ne * a33;
+            }
+            // outputs: 0 G_x = conv_x + i kz t13, 1 G_y, 2 G_z, 3 t11, 4 t12, 5 t13, 6 t22, 7 t23
+#pragma unroll
+            for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(cxv[e], PH(6, row)); }
+            k3_store_pair<T, L, E>(A, sm, q, g.Kz, F[0], F[5], true, sz, ok, tw);
+#pragma unroll
+            for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(cyv[e], PH(7, row)); }
+            k3_store_pair<T, L, E>(A, sm, q, g.Kz, F[1], F[7], true, sz, ok, tw);
+#pragma unroll
+            for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(czv[e], PH(8, row)); }
+            k3_store_pair<T, L, E>(A, sm, q, g.Kz, F[2], nullptr, true, sz, ok, tw);
+#pragma unroll
+            for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(PH(3, row), PH(4, row)); }
+            k3_store_pair<T, L, E>(A, sm, q, g.Kz, F[3], F[4], false, sz, ok, tw);
+#pragma unroll
+            for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(PH(5, row), T(0)); }
+            k3_store_single<T, L, E>(A, sm, q, g.Kz, F[6], ok, tw);
+        }
+    }
+}
+
+// ===========================================================================
+// K4: forward transform along y with ky truncation.  Block = (kz chunk, x).
+// LES: G_i += i ky t_i2 (SGS divergence, y part).
+// ===========================================================================
+template <typename T, int L, int E, int P, int MODE>
+__global__ void __launch_bounds__(P *(L / E)) k4_fwd_y(Geo g, const cx<T> *__restrict__ in, cx<T> *__restrict__ out,
+                                                       const cx<T> *__restrict__ tw) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int tid = threadIdx.x, p = tid % P, q = tid / P;
+    const int x = blockIdx.y, kz = blockIdx.x * P + p;
+    const bool ok = kz < g.Kz;
+    SmRowMajor<T, P> sm{reinterpret_cast<cx<T> *>(smraw), p};
+    const long long col = (long long)x * g.Kz + kz;
+    auto load_fft = [&](cx<T>(&r)[E], int f) {
+        const cx<T> *src = in + (long long)f * g.S2 + col;
+#pragma unroll
+        for (int e = 0; e < E; e++) r[e] = ok ? src[(long long)in_row<L, E, false>(q, e) * g.Mx * g.Kz] : zero<T>();
+        fft<T, L, E, false>(r, sm, q, tw);
+    };
+    auto store = [&](const cx<T>(&r)[E], int f, const cx<T> *add, bool use_add) {
+        if (!ok) return;
+        cx<T> *o = out + (long long)f * g.S1 + col;
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+            const int m2 = ffreq(out_row<L, E, false>(q, e), L);
+            if (m2 <= g.hy && m2 >= -g.hy) {
+                cx<T> val = r[e];
+                if (use_add) val = val + mul_i(T(g.sy * m2) * add[e]);
+                o[(long long)(m2 >= 0 ? m2 : m2 + g.Ky) * g.Mx * g.Kz] = val;
+            }
+        }
+    };
+    if constexpr (MODE != MODE_LES) {
+#pragma unroll 1
+        for (int f = 0; f < 3; f++) {
+            cx<T> r[E];
+            load_fft(r, f);
+            store(r, f, r, false);
+        }
+    } else {
+        // in (S2): 0 G_x, 1 G_y, 2 G_z, 3 t11, 4 t12, 5 t13, 6 t22, 7 t23
+        // out (S1): 0 G_x + i ky t12, 1 G_y + i ky t22, 2 G_z + i ky t23, 3 t11, 4 t12, 5 t13
+        const int gi[3] = {0, 1, 2}, ti[3] = {4, 6, 7};
+#pragma unroll 1
+        for (int i = 0; i < 3; i++) {
+            cx<T> r[E], t[E];
+            load_fft(r, gi[i]);
+            load_fft(t, ti[i]);
+            store(r, i, t, true);
+            if (i == 0) store(t, 4, t, false);
+        }
+#pragma unroll 1
+        for (int f = 3; f <= 5; f += 2) {
+            cx<T> r[E];
+            load_fft(r, f);
+            store(r, f, r, false);
+        }
+    }
+}
+
+// ===========================================================================
+// K5: forward transform along x + the spectral sweep of the step
+// (src/HIT_LES.cpp:196-242 R vector, 243-278 constant-power forcing,
+//  295-339 predictor, 346-359 projection).  Block = (kz chunk, iy).
+// LES: G_i += i kx t_i1 (SGS divergence, x part).
+// ===========================================================================
+template <typename T, int L, int E, int P, int MODE, bool SELF>
+__global__ void __launch_bounds__(P *(L / E)) k5_fwd_x_sweep(Geo g, const cx<T> *__restrict__ in, cx<T> *__restrict__ U,
+                                                             cx<T> *__restrict__ R, cx<T> *__restrict__ Uprev,
+                                                             StepConsts c, const DevScalars *__restrict__ ds,
+                                                             const cx<T> *__restrict__ tw) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int tid = threadIdx.x, p = tid % P, q = tid / P;
+    const int iy = blockIdx.y, kz = blockIdx.x * P + p;
+    const bool ok = kz < g.Kz;
+    SmRowMajor<T, P> sm{reinterpret_cast<cx<T> *>(smraw), p};
+    cx<T> G[3][E];
+    const long long col = (long long)iy * g.Mx * g.Kz + kz;
+#pragma unroll
+    for (int f = 0; f < 3; f++) {
+        const cx<T> *src = in + (long long)f * g.S1 + col;
+#pragma unroll
+        for (int e = 0; e < E; e++) G[f][e] = ok ? src[(long long)in_row<L, E, false>(q, e) * g.Kz] : zero<T>();
+        fft<T, L, E, false>(G[f], sm, q, tw);
+        if constexpr (MODE == MODE_LES) {
+            cx<T> t[E];
+            const cx<T> *ts = in + (long long)(3 + f) * g.S1 + col;
+#pragma unroll
+            for (int e = 0; e < E; e++) t[e] = ok ? ts[(long long)in_row<L, E, false>(q, e) * g.Kz] : zero<T>();
+            fft<T, L, E, false>(t, sm, q, tw);
+#pragma unroll
+            for (int e = 0; e < E; e++) {
+                const int m1 = ffreq(out_row<L, E, false>(q, e), L);
+                G[f][e] = G[f][e] + mul_i(T(g.sx * m1) * t[e]);
+            }
+        }
+    }
+    if (!ok) return;
+    const double nu = ds->nu, dt = ds->dt, kap = ds->kappa, alpha = ds->alpha;
+    const bool first = ds->iter == 0;
+    const int m2 = iy <= g.hy ? iy : iy - g.Ky;
+    const long long k2 = (long long)g.sy * m2, k3 = (long long)g.sz * kz;
+    const long long S0 = g.S0;
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+        const int m1 = ffreq(out_row<L, E, false>(q, e), L);
+        if (m1 > g.hx || m1 < -g.hx) continue;
+        const long long idx = ((long long)iy * g.Kx + (m1 >= 0 ? m1 : m1 + g.Kx)) * g.Kz + kz;
+        const long long k1 = (long long)g.sx * m1;
+        const double rad2 = (double)(k1 * k1 + k2 * k2 + k3 * k3);
+        const bool mean = !(rad2 > 0.0);
+        const double ct = nu * rad2;
+        double ur[3], ui[3], rr[3], ri[3];
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            const cx<T> uu = U[i * S0 + idx];
+            ur[i] = uu.x; ui[i] = uu.y;
+            const double gr = mean ? 0.0 : (double)G[i][e].x * c.inv_norm;
+            const double gi = mean ? 0.0 : (double)G[i][e].y * c.inv_norm;
+            rr[i] = -gr - ct * ur[i];
+            ri[i] = -gi - ct * ui[i];
+        }
+        if (c.rotating) {
+            rr[0] += 2 * (c.omega_z * ur[1] - c.omega_y * ur[2]); ri[0] += 2 * (c.omega_z * ui[1] - c.omega_y * ui[2]);
+            rr[1] += 2 * (c.omega_x * ur[2] - c.omega_z * ur[0]); ri[1] += 2 * (c.omega_x * ui[2] - c.omega_z * ui[0]);
+            rr[2] += 2 * (c.omega_y * ur[0] - c.omega_x * ur[1]); ri[2] += 2 * (c.omega_y * ui[0] - c.omega_x * ui[1]);
+        }
+        if (c.eps_on) {
+            const int K = (int)round(sqrt(rad2));
+            if (c.eps_kmin <= K && K <= c.eps_kmax) {
+#pragma unroll
+                for (int i = 0; i < 3; i++) { rr[i] += alpha * ur[i]; ri[i] += alpha * ui[i]; }
+            } else if (K == 0) {
+#pragma unroll
+                for (int i = 0; i < 3; i++) { rr[i] = 0.0; ri[i] = 0.0; }
+            }
+        }
+        double sr[3], si[3];
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            const cx<T> r0 = R[i * S0 + idx];
+            if (SELF) {
+                double pr = ur[i], pi = ui[i];
+                if (!first) { const cx<T> up = Uprev[i * S0 + idx]; pr = up.x; pi = up.y; }
+                const double k05 = 1.0 / (kap + 0.5);
+                sr[i] = k05 * (2.0 * kap * ur[i] + dt * ((1.0 + kap) * rr[i] - kap * (double)r0.x) - (kap - 0.5) * pr);
+                si[i] = k05 * (2.0 * kap * ui[i] + dt * ((1.0 + kap) * ri[i] - kap * (double)r0.y) - (kap - 0.5) * pi);
+                Uprev[i * S0 + idx] = mk<T>(T(ur[i]), T(ui[i]));
+            } else {
+                sr[i] = ur[i] + dt * (1.5 * rr[i] - 0.5 * (double)r0.x);
+                si[i] = ui[i] + dt * (1.5 * ri[i] - 0.5 * (double)r0.y);
+            }
+            R[i * S0 + idx] = mk<T>(T(rr[i]), T(ri[i]));
+        }
+        if (rad2 > 0.0) {
+            const double kk[3] = {(double)k1, (double)k2, (double)k3};
+            const double ar = (kk[0] * sr[0] + kk[1] * sr[1] + kk[2] * sr[2]) / rad2;
+            const double ai = (kk[0] * si[0] + kk[1] * si[1] + kk[2] * si[2]) / rad2;
+#pragma unroll
+            for (int i = 0; i < 3; i++) { sr[i] -= ar * kk[i]; si[i] -= ai * kk[i]; }
+        }
+#pragma unroll
+        for (int i = 0; i < 3; i++) U[i * S0 + idx] = mk<T>(T(sr[i]), T(si[i]));
+    }
+}
+
+// ===========================================================================
+// Small kernels
+// ===========================================================================
+__device__ __forceinline__ double Topt_d(const StepConsts &c, double phi0, int *err) {
+    const double PI_ = 3.141592653589793238462643;
+    auto FuL = [](double x, double x0, double x1, double f0, double f1) { return f0 + (x - x0) * (f1 - f0) / (x1 - x0); };
+    auto FuG = [&](double x, double a, double b, double cc, double x0, double x1, double f0, double f1) {
+        return (a * x * x + b * x + cc) * ((x - x0) * (x - x1)) + FuL(x, x0, x1, f0, f1);
+    };
+    if (phi0 >= 0.0 && phi0 < c.phi[0]) return FuG(phi0, 0.0, c.c[0], c.c[1], 0.0, c.phi[0], 4.0 / 3.0, c.t1);
+    if (phi0 >= c.phi[0] && phi0 <= PI_ / 2.0) return FuG(phi0, c.c[2], c.c[3], c.c[4], c.phi[0], PI_ / 2.0, c.t1, 1.0);
+    *err = 1;
+    return 0.0;
+}
+__device__ __forceinline__ double Kopt_d(const StepConsts &c, double phi0, int *err) {
+    const double PI_ = 3.141592653589793238462643;
+    auto FuL = [](double x, double x0, double x1, double f0, double f1) { return f0 + (x - x0) * (f1 - f0) / (x1 - x0); };
+    auto FuG = [&](double x, double a, double b, double cc, double x0, double x1, double f0, double f1) {
+        return (a * x * x + b * x + cc) * ((x - x0) * (x - x1)) + FuL(x, x0, x1, f0, f1);
+    };
+    if (phi0 >= 0.0 && phi0 <= c.phi[0]) return 1.0;
+    if (phi0 > c.phi[0] && phi0 <= c.phi[1]) return FuG(phi0, c.c[5], c.c[6], c.c[7], c.phi[0], c.phi[1], 1.0, c.kopt_k[0]);
+    if (phi0 > c.phi[1] && phi0 <= c.phi[2]) return FuG(phi0, c.c[8], c.c[9], c.c[10], c.phi[1], c.phi[2], c.kopt_k[0], c.kopt_k[1]);
+    if (phi0 > c.phi[2] && phi0 <= PI_ / 2.0) return FuG(phi0, c.c[11], c.c[12], c.c[13], c.phi[2], PI_ / 2.0, c.kopt_k[1], 0.0);
+    *err = 1;
+    return 0.0;
+}
+
+// src/HIT_LES.cpp:365-403, from the maxima gathered by the last inverse transform.
+__device__ __forceinline__ void recalc_dt(const StepConsts &c, DevScalars *ds) {
+    if (c.fixed_dt > 0.0) { ds->dt = c.fixed_dt; return; }
+    const double nu = ds->nu;
+    if (c.self_adaptive) {
+        const double MaxVel = __longlong_as_double((long long)ds->max_bits[3]);
+        ds->maxvel = MaxVel;
+        const double Ah = c.Ah;
+        const double phi0 = atan(MaxVel * Ah * Ah / (0.35 * nu * 12.0));
+        ds->phi0 = phi0;
+        int err = 0;
+        double At = Topt_d(c, phi0, &err) / sqrt((MaxVel * MaxVel) / (0.35 * 0.35) + (144.0 * nu * nu / (Ah * Ah * Ah * Ah)));
+        ds->kappa = Kopt_d(c, phi0, &err);
+        if (err) ds->domain_err = 1;
+        ds->dt = c.C_At * At;
+    } else {
+        const double mu = __longlong_as_double((long long)ds->max_bits[0]);
+        const double mv = __longlong_as_double((long long)ds->max_bits[1]);
+        const double mw = __longlong_as_double((long long)ds->max_bits[2]);
+        const double MaxVel = fmax(mu / c.Ax, fmax(mv / c.Ay, mw / c.Az));
+        ds->maxvel = MaxVel;
+        const double C_visc = 0.2 * fmin(c.Ax * c.Ax, fmin(c.Ay * c.Ay, c.Az * c.Az)) / nu;
+        const double C_conv = 0.35 / MaxVel;
+        ds->dt = c.C_At * fmin(C_visc, C_conv);
+    }
+}
+
+__global__ void k_recalc_dt(StepConsts c, DevScalars *ds) { recalc_dt(c, ds); }
+
+// End of New_Fractional_Step_Method (src/HIT_LES.cpp:19-24).
+__global__ void k_finish_step(StepConsts c, DevScalars *ds) {
+    recalc_dt(c, ds);
+    ds->time = ds->time + ds->dt;
+    ds->iter += 1;
+}
+
+__global__ void k_reset_max(DevScalars *ds) {
+    for (int i = 0; i < 4; i++) ds->max_bits[i] = 0ull;
+    ds->sumsq_phys = 0.0;
+}
+
+// Shell sums of the spectral state (src/HIT_LES.cpp:1137-1214 with the
+// KineticEnergy and Enstrophy integrands of :991-1003).  Modes with kz>0 carry
+// their conjugate (weight 2).  Ek[K], Om[K] for K=round(|k|) <= Kmax.
+template <typename T>
+__global__ void k_shell_sums(Geo g, const cx<T> *__restrict__ u, const cx<T> *__restrict__ v, const cx<T> *__restrict__ w,
+                             int Kmax, double *__restrict__ Ek, double *__restrict__ Om) {
+    extern __shared__ double hist[];
+    double *hE = hist, *hO = hist + (Kmax + 1);
+    for (int i = threadIdx.x; i < 2 * (Kmax + 1); i += blockDim.x) hist[i] = 0.0;
+    __syncthreads();
+    const long long n = g.S0;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long long)gridDim.x * blockDim.x) {
+        const int kz = (int)(idx % g.Kz);
+        const long long t = idx / g.Kz;
+        const int ix = (int)(t % g.Kx), iy = (int)(t / g.Kx);
+        const long long k1 = (long long)g.sx * (ix <= g.hx ? ix : ix - g.Kx);
+        const long long k2 = (long long)g.sy * (iy <= g.hy ? iy : iy - g.Ky);
+        const long long k3 = (long long)g.sz * kz;
+        const double rad2 = (double)(k1 * k1 + k2 * k2 + k3 * k3);
+        const int K = (int)round(sqrt(rad2));
+        if (K > Kmax) continue;
+        const cx<T> a = u[idx], b = v[idx], cc = w[idx];
+        double e = 0.5 * ((double)a.x * a.x + (double)a.y * a.y + (double)b.x * b.x + (double)b.y * b.y + (double)cc.x * cc.x +
+                          (double)cc.y * cc.y);
+        if (kz != 0) e *= 2.0;
+        atomicAdd(&hE[K], e);
+        atomicAdd(&hO[K], 2.0 * rad2 * e);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i <= Kmax; i += blockDim.x) {
+        if (hE[i] != 0.0) atomicAdd(&Ek[i], hE[i]);
+        if (hO[i] != 0.0) atomicAdd(&Om[i], hO[i]);
+    }
+}
+
+// Totals of the shell sums: Ek_Tot over K=0..Kmax, Ok_Tot over K=1..Kmax.
+// what: 0 energy only, 1 energy+enstrophy (+ReLambda), 2 Forcing_Reynolds_Lambda.
+__global__ void k_totals(const double *Ek, const double *Om, int Kmax, DevScalars *ds, int what, double relambda) {
+    double e = 0.0, o = 0.0;
+    for (int K = 0; K <= Kmax; K++) e += Ek[K];
+    for (int K = 1; K <= Kmax; K++) o += Om[K];
+    ds->ek_tot = e;
+    if (what >= 1) ds->ok_tot = o;
+    if (what == 1) ds->relambda = e / ds->nu * sqrt(20.0 / 3.0 / o);
+    if (what == 2) ds->nu = e / relambda * sqrt(20.0 / 3.0 / o);
+}
+
+// Constant-power forcing coefficient alpha = eps/(2 E_f), E_f the energy of
+// shells [kmin,kmax] of the current state (src/HIT_LES.cpp:250-256).
+__global__ void k_eps_alpha(const double *Ek, int kmin, int kmax, double eps, DevScalars *ds) {
+    double Ef = 0.0;
+    for (int K = kmin; K <= kmax; K++) Ef += Ek[K];
+    ds->alpha = Ef > 1e-30 ? eps / (2.0 * Ef) : 0.0;
+}
+
+// src/HIT_LES.cpp:417-419: FT[K] = sqrt(Forced_Ek[K]/Ek[K]).
+__global__ void k_forcing_factors(const double *Ek, const double *Forced, int last_eff, double *FT) {
+    for (int K = threadIdx.x; K <= last_eff; K += blockDim.x) FT[K] = Ek[K] > 0.0 ? sqrt(Forced[K] / Ek[K]) : 0.0;
+}
+
+// src/HIT_LES.cpp:421-438: scale shells K<=last_eff, optionally zero the rest.
+template <typename T>
+__global__ void k_forcing_scale(Geo g, cx<T> *u, cx<T> *v, cx<T> *w, const double *FT, int last_eff, int nullify) {
+    const long long n = g.S0;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long long)gridDim.x * blockDim.x) {
+        const int kz = (int)(idx % g.Kz);
+        const long long t = idx / g.Kz;
+        const int ix = (int)(t % g.Kx), iy = (int)(t / g.Kx);
+        const long long k1 = (long long)g.sx * (ix <= g.hx ? ix : ix - g.Kx);
+        const long long k2 = (long long)g.sy * (iy <= g.hy ? iy : iy - g.Ky);
+        const long long k3 = (long long)g.sz * kz;
+        const int K = (int)round(sqrt((double)(k1 * k1 + k2 * k2 + k3 * k3)));
+        if (K <= last_eff) {
+            const T f = T(FT[K]);
+            u[idx] = f * u[idx]; v[idx] = f * v[idx]; w[idx] = f * w[idx];
+        } else if (nullify) {
+            u[idx] = zero<T>(); v[idx] = zero<T>(); w[idx] = zero<T>();
+        }
+    }
+}
+
+// src/HIT_LES.cpp:446-476 on the kz=0 plane: u(k1<0 or k1=0,k2<0) = conj(u(-k)).
+// The written and the read halves are disjoint, so no staging copy is needed.
+template <typename T>
+__global__ void k_conj_correction(Geo g, cx<T> *u, cx<T> *v, cx<T> *w) {
+    const int n = g.Kx * g.Ky;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const int ix = t % g.Kx, iy = t / g.Kx;
+        const int m1 = ix <= g.hx ? ix : ix - g.Kx, m2 = iy <= g.hy ? iy : iy - g.Ky;
+        if (m1 < 0 || (m1 == 0 && m2 < 0)) {
+            const int jx = -m1, jy = -m2 >= 0 ? -m2 : -m2 + g.Ky;
+            const long long dst = ((long long)iy * g.Kx + ix) * g.Kz, src = ((long long)jy * g.Kx + jx) * g.Kz;
+            u[dst] = conj(u[src]); v[dst] = conj(v[src]); w[dst] = conj(w[src]);
+        }
+    }
+}
+
+// Direct DFT along one axis (initial-field transform of the input file; init only).
+// in: complex lines, out: complex lines; out[o][k] = sum_n in[o][n] * w^(k*n mod N).
+// Line l of `nl` lines starts at (l / inner)*outer_stride + (l % inner), element stride `es`.
+__global__ void k_dft_axis(const double2 *__restrict__ in, double2 *__restrict__ out, int N, int nk, const int *__restrict__ kidx,
+                           long long nl, long long inner, long long in_outer, long long out_outer, long long es_in,
+                           long long es_out, const double2 *__restrict__ twN) {
+    const long long tot = nl * nk;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
+        const int kk = (int)(t % nk);
+        const long long l = t / nk;
+        const long long ib = (l / inner) * in_outer + (l % inner), ob = (l / inner) * out_outer + (l % inner);
+        const int k = kidx[kk];
+        double sr = 0.0, si = 0.0;
+        long long m = 0;
+        for (int n = 0; n < N; n++) {
+            const double2 a = in[ib + n * es_in], wv = twN[m];
+            sr += a.x * wv.x - a.y * wv.y;
+            si += a.x * wv.y + a.y * wv.x;
+            m += k; if (m >= N) m -= N;
+        }
+        out[ob + (long long)kk * es_out] = make_double2(sr, si);
+    }
+}
+
+} // namespace spns

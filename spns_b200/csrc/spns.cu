@@ -1,0 +1,902 @@
+// spns.cu -- libspns: handle management, launch dispatch and the C ABI (include/spns.h).
+//
+// Every entry point forwards one member of the reference class HIT
+// (src/HIT_LES.h of adalbal/SpNS); see include/spns.h for the mapping.
+#include "spns.h"
+#include "solver_kernels.cuh"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+using namespace spns;
+
+// ---------------------------------------------------------------------------
+// Compiled FFT lengths and launch shapes
+// ---------------------------------------------------------------------------
+#define SPNS_FOR_EACH_LENGTH(X) X(48) X(72) X(96) X(144) X(192) X(288) X(384) X(768) X(1536)
+
+static bool length_supported(int L) {
+#define SPNS_CASE(n) if (L == n) return true;
+    SPNS_FOR_EACH_LENGTH(SPNS_CASE)
+#undef SPNS_CASE
+    return false;
+}
+
+template <typename T, int L> struct Shape {
+    static constexpr int E = 12;             // complex values per thread
+    static constexpr int Q = L / E;          // threads per pencil
+    static constexpr int P0 = 256 / Q;
+    static constexpr int P = P0 >= 32 ? 32 : P0 >= 16 ? 16 : P0 >= 8 ? 8 : 4; // pencils per block
+    static constexpr int THREADS = P * Q;
+    static constexpr size_t SMEM_ROW = (size_t)L * P * sizeof(cx<T>);
+    static constexpr size_t SMEM_PEN = (size_t)SmPencil<T, L>::PITCH * P * sizeof(cx<T>);
+};
+
+// z pass: pencils per block limited by the shared memory of the exchange
+// buffer plus the physical fields kept per pencil.
+template <typename T, int L, int MODE> struct Shape3 {
+    using S = Shape<T, L>;
+    static constexpr size_t PER_PEN = (size_t)SmPencil<T, L>::PITCH * sizeof(cx<T>) + (size_t)K3Phys<MODE>::N * L * sizeof(T);
+    static constexpr int PMAX = (int)((200 * 1024) / PER_PEN);
+    static constexpr int P = S::P <= PMAX ? S::P : PMAX >= 16 ? 16 : PMAX >= 8 ? 8 : PMAX >= 4 ? 4 : PMAX >= 2 ? 2 : 1;
+    static constexpr int THREADS = P * S::Q;
+    static constexpr size_t SMEM = PER_PEN * P;
+};
+
+// ---------------------------------------------------------------------------
+// Handle
+// ---------------------------------------------------------------------------
+struct spns_handle {
+    spns_hit_args a;
+    Geo g;
+    StepConsts c;
+    int last_rad = 0, last_rad_max = 0;
+    double delta = 0, Ek_init = 0, Ek_init_file = 0, Enstrophy_init_file = 0;
+    cudaStream_t st = nullptr;
+    DevScalars *ds = nullptr;
+    double2 *U = nullptr, *R = nullptr, *Up = nullptr; // 3 fields each (S0)
+    double2 *B1 = nullptr, *B2 = nullptr;            // S1 and S2 work buffers
+    int nB1 = 0, nB2 = 0;
+    double *bins = nullptr;                          // Ek[0..Kmax], Om[0..Kmax]
+    double *FT = nullptr, *forced = nullptr;
+    int forced_cap = 0;
+    double *phys = nullptr;
+    std::map<int, double2 *> tw;                     // twiddle tables per length
+    std::string err;
+    int kernels_per_step = 0;
+    // optional per-kernel event profile of the next steps (spns_profile_*)
+    std::vector<cudaEvent_t> prof_ev;
+    std::vector<std::string> prof_names;
+    int prof_cap_steps = 0, prof_steps = 0, prof_nk = 0;
+};
+
+static thread_local std::string g_create_error;
+
+static int fail(spns_handle *h, int code, const char *fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (h) h->err = buf; else g_create_error = buf;
+    return code;
+}
+
+#define CK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return fail(h, e_ == cudaErrorMemoryAllocation ? SPNS_ERR_OUT_OF_MEMORY : SPNS_ERR_CUDA, \
+                        "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+#define CKL()                                                                                      \
+    do {                                                                                           \
+        cudaError_t e_ = cudaGetLastError();                                                       \
+        if (e_ != cudaSuccess)                                                                     \
+            return fail(h, SPNS_ERR_CUDA, "kernel launch failed: %s (%s:%d)", cudaGetErrorString(e_), \
+                        __FILE__, __LINE__);                                                       \
+    } while (0)
+
+static int actual_n(int n, int L) { return (n % 2 == 0) ? n / L : (n - 1) / L + 1; }
+
+static double2 *make_twiddles(int L) {
+    std::vector<double2> t(L);
+    for (int m = 0; m < L; m++) {
+        long double ang = 2.0L * 3.14159265358979323846264338327950288L * (long double)m / (long double)L;
+        t[m] = make_double2((double)cosl(ang), (double)(-sinl(ang)));
+    }
+    double2 *d = nullptr;
+    if (cudaMalloc(&d, sizeof(double2) * L) != cudaSuccess) return nullptr;
+    if (cudaMemcpy(d, t.data(), sizeof(double2) * L, cudaMemcpyHostToDevice) != cudaSuccess) { cudaFree(d); return nullptr; }
+    return d;
+}
+
+template <class K> static cudaError_t set_smem(K kern, size_t bytes) {
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+// ---------------------------------------------------------------------------
+// Typed launchers (FP64 plain form)
+// ---------------------------------------------------------------------------
+using T64 = double;
+
+template <int L, int MODE> static cudaError_t launch_k1(spns_handle *h) {
+    using S = Shape<T64, L>;
+    auto kern = k1_inv_x<T64, L, S::E, S::P, MODE>;
+    cudaError_t e = set_smem(kern, S::SMEM_ROW);
+    if (e != cudaSuccess) return e;
+    dim3 grid((h->g.Kz + S::P - 1) / S::P, h->g.Ky);
+    kern<<<grid, S::THREADS, S::SMEM_ROW, h->st>>>(h->g, (const cx<T64> *)h->U, (const cx<T64> *)(h->U + h->g.S0),
+                                                  (const cx<T64> *)(h->U + 2 * h->g.S0), (cx<T64> *)h->B1,
+                                                  (const cx<T64> *)h->tw[L]);
+    return cudaGetLastError();
+}
+template <int L, int MODE> static cudaError_t launch_k2(spns_handle *h) {
+    using S = Shape<T64, L>;
+    auto kern = k2_inv_y<T64, L, S::E, S::P, MODE>;
+    cudaError_t e = set_smem(kern, S::SMEM_ROW);
+    if (e != cudaSuccess) return e;
+    dim3 grid((h->g.Kz + S::P - 1) / S::P, h->g.Mx);
+    kern<<<grid, S::THREADS, S::SMEM_ROW, h->st>>>(h->g, (const cx<T64> *)h->B1, (cx<T64> *)h->B2, (const cx<T64> *)h->tw[L]);
+    return cudaGetLastError();
+}
+template <int L, int MODE> static cudaError_t launch_k3(spns_handle *h, double *phys) {
+    using S = Shape<T64, L>;
+    using S3 = Shape3<T64, L, MODE>;
+    auto kern = k3_z<T64, L, S::E, S3::P, MODE>;
+    cudaError_t e = set_smem(kern, S3::SMEM);
+    if (e != cudaSuccess) return e;
+    const long long npen = (long long)h->g.Mx * h->g.My;
+    dim3 grid((unsigned)((npen + S3::P - 1) / S3::P));
+    kern<<<grid, S3::THREADS, S3::SMEM, h->st>>>(h->g, (cx<T64> *)h->B2, h->c, h->ds, phys, (const cx<T64> *)h->tw[L]);
+    return cudaGetLastError();
+}
+template <int L, int MODE> static cudaError_t launch_k4(spns_handle *h) {
+    using S = Shape<T64, L>;
+    auto kern = k4_fwd_y<T64, L, S::E, S::P, MODE>;
+    cudaError_t e = set_smem(kern, S::SMEM_ROW);
+    if (e != cudaSuccess) return e;
+    dim3 grid((h->g.Kz + S::P - 1) / S::P, h->g.Mx);
+    kern<<<grid, S::THREADS, S::SMEM_ROW, h->st>>>(h->g, (const cx<T64> *)h->B2, (cx<T64> *)h->B1, (const cx<T64> *)h->tw[L]);
+    return cudaGetLastError();
+}
+template <int L, int MODE, bool SELF> static cudaError_t launch_k5(spns_handle *h) {
+    using S = Shape<T64, L>;
+    auto kern = k5_fwd_x_sweep<T64, L, S::E, S::P, MODE, SELF>;
+    cudaError_t e = set_smem(kern, S::SMEM_ROW);
+    if (e != cudaSuccess) return e;
+    dim3 grid((h->g.Kz + S::P - 1) / S::P, h->g.Ky);
+    kern<<<grid, S::THREADS, S::SMEM_ROW, h->st>>>(h->g, (const cx<T64> *)h->B1, (cx<T64> *)h->U, (cx<T64> *)h->R,
+                                                  (cx<T64> *)h->Up, h->c, h->ds, (const cx<T64> *)h->tw[L]);
+    return cudaGetLastError();
+}
+
+#define DISPATCH(Lval, call)                                                                 \
+    switch (Lval) {                                                                          \
+    case 48: { constexpr int LL = 48; call; } break;                                         \
+    case 72: { constexpr int LL = 72; call; } break;                                         \
+    case 96: { constexpr int LL = 96; call; } break;                                         \
+    case 144: { constexpr int LL = 144; call; } break;                                       \
+    case 192: { constexpr int LL = 192; call; } break;                                       \
+    case 288: { constexpr int LL = 288; call; } break;                                       \
+    case 384: { constexpr int LL = 384; call; } break;                                       \
+    case 768: { constexpr int LL = 768; call; } break;                                       \
+    case 1536: { constexpr int LL = 1536; call; } break;                                     \
+    default: return fail(h, SPNS_ERR_UNSUPPORTED_SIZE, "FFT length %d is not compiled", Lval); \
+    }
+
+#define LAUNCH(expr)                                                                              \
+    do {                                                                                          \
+        cudaError_t e_ = (expr);                                                                  \
+        if (e_ != cudaSuccess)                                                                    \
+            return fail(h, SPNS_ERR_CUDA, "launch failed: %s (%s:%d)", cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+// Inverse transform of the velocity only (Recalculate_Velocity_Antitransform):
+// refreshes the CFL maxima and, if phys != NULL, writes u,v,w on the grid.
+static int run_velocity(spns_handle *h, double *phys) {
+    k_reset_max<<<1, 1, 0, h->st>>>(h->ds);
+    CKL();
+    DISPATCH(h->g.Mx, LAUNCH((launch_k1<LL, MODE_VEL>(h))));
+    DISPATCH(h->g.My, LAUNCH((launch_k2<LL, MODE_VEL>(h))));
+    DISPATCH(h->g.Mz, LAUNCH((launch_k3<LL, MODE_VEL>(h, phys))));
+    return SPNS_OK;
+}
+
+static int shell_sums(spns_handle *h, int bx, int by, int bz) {
+    (void)bx; (void)by; (void)bz;
+    const int nb = h->last_rad_max + 1;
+    CK(cudaMemsetAsync(h->bins, 0, sizeof(double) * 2 * nb, h->st));
+    const long long n = h->g.S0;
+    int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 8);
+    k_shell_sums<T64><<<blocks, 256, sizeof(double) * 2 * nb, h->st>>>(
+        h->g, (const cx<T64> *)h->U, (const cx<T64> *)(h->U + h->g.S0), (const cx<T64> *)(h->U + 2 * h->g.S0), h->last_rad_max,
+        h->bins, h->bins + nb);
+    CKL();
+    return SPNS_OK;
+}
+
+// Records an event before the next kernel of a profiled step.
+static void prof_mark(spns_handle *h, int slot, const char *name) {
+    if (h->prof_steps >= h->prof_cap_steps) return;
+    if (slot >= 16) return;
+    if (h->prof_steps == 0 && (int)h->prof_names.size() <= slot) h->prof_names.push_back(name ? name : "");
+    cudaEventRecord(h->prof_ev[(size_t)h->prof_steps * 16 + slot], h->st);
+}
+
+static int step_once(spns_handle *h) {
+    int nk = 0;
+    int slot = 0;
+    const bool prof = h->prof_steps < h->prof_cap_steps;
+#define MARK(name) do { if (prof) prof_mark(h, slot++, name); } while (0)
+    if (h->a.eps_forcing > 0.0) {
+        MARK("shell_sums");
+        int r = shell_sums(h, 0, 0, 0);
+        if (r) return r;
+        MARK("eps_alpha");
+        k_eps_alpha<<<1, 1, 0, h->st>>>(h->bins, h->a.eps_kmin, h->a.eps_kmax, h->a.eps_forcing, h->ds);
+        CKL();
+        nk += 2;
+    }
+    const int mode = h->a.isLES ? MODE_LES : h->a.nonlinear_form == 1 ? MODE_ROT : MODE_ADV;
+#define STEP_PASSES(MD)                                                                       \
+    MARK("k1_inv_x");                                                                         \
+    DISPATCH(h->g.Mx, LAUNCH((launch_k1<LL, MD>(h))));                                        \
+    MARK("k2_inv_y");                                                                         \
+    DISPATCH(h->g.My, LAUNCH((launch_k2<LL, MD>(h))));                                        \
+    MARK("reset_max");                                                                        \
+    k_reset_max<<<1, 1, 0, h->st>>>(h->ds);                                                   \
+    CKL();                                                                                    \
+    MARK("k3_z");                                                                             \
+    DISPATCH(h->g.Mz, LAUNCH((launch_k3<LL, MD>(h, nullptr))));                               \
+    MARK("k4_fwd_y");                                                                         \
+    DISPATCH(h->g.My, LAUNCH((launch_k4<LL, MD>(h))));                                        \
+    MARK("k5_fwd_x_sweep");                                                                   \
+    if (h->a.isSelfAdaptive) { DISPATCH(h->g.Mx, LAUNCH((launch_k5<LL, MD, true>(h)))); }     \
+    else { DISPATCH(h->g.Mx, LAUNCH((launch_k5<LL, MD, false>(h)))); }
+    if (mode == MODE_LES) { STEP_PASSES(MODE_LES) }
+    else if (mode == MODE_ROT) { STEP_PASSES(MODE_ROT) }
+    else { STEP_PASSES(MODE_ADV) }
+#undef STEP_PASSES
+    MARK("finish_step");
+    k_finish_step<<<1, 1, 0, h->st>>>(h->c, h->ds);
+    CKL();
+    MARK(nullptr);
+    if (prof) { if (h->prof_steps == 0) h->prof_nk = slot - 1; h->prof_steps++; }
+    h->kernels_per_step = nk + 7;
+    return SPNS_OK;
+#undef MARK
+}
+
+static int check_flags(spns_handle *h) {
+    DevScalars s;
+    CK(cudaMemcpyAsync(&s, h->ds, sizeof(s), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    if (s.nonfinite) return fail(h, SPNS_ERR_NONFINITE, "non-finite velocity met in the CFL maximum (iter %lld)", s.iter);
+    if (s.domain_err) return fail(h, SPNS_ERR_DOMAIN, "Topt fail! (time-step angle outside [0, pi/2])");
+    return SPNS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Initial fields
+// ---------------------------------------------------------------------------
+// K41 field (src/HIT_LES.cpp:502-525) generated on the host in the reference's
+// loop order, rank by rank (srand(0) per rank, FFTW-MPI block of the transposed
+// dimension), written into the compact layout.
+static void k41_host(const spns_handle *h, std::vector<double2> &uvw) {
+    const spns_hit_args &a = h->a;
+    const Geo &g = h->g;
+    const int Mx = a.Mx, My = a.My, Mz2 = a.Mz / 2;
+    const int Nx2 = a.Nx / 2, Ny2 = a.Ny / 2, Nz2 = a.Nz / 2;
+    const int P = a.k41_ranks > 0 ? a.k41_ranks : 1;
+    const int blk = (My + P - 1) / P;
+    uvw.assign(3 * (size_t)g.S0, make_double2(0.0, 0.0));
+    for (int r = 0; r < P; r++) {
+        const int b0 = r * blk, b1 = std::min(My, (r + 1) * blk);
+        srand(0);
+        for (int b = b0; b < b1; b++) {
+            const int k2 = b <= My / 2 ? b : b - My;
+            for (int aa = 0; aa < Mx; aa++) {
+                const int k1 = aa <= Mx / 2 ? aa : aa - Mx;
+                for (int k3 = 0; k3 <= Mz2; k3++) {
+                    bool d = std::abs(k1) <= Nx2 && std::abs(k2) <= Ny2 && k3 <= Nz2;
+                    if (a.isNotCubic && ((k1 % a.Lx_factor) != 0 || (k2 % a.Ly_factor) != 0 || (k3 % a.Lz_factor) != 0)) d = false;
+                    if (!d) continue;
+                    const int K = (int)std::round(std::sqrt((double)(k1 * k1 + k2 * k2 + k3 * k3)));
+                    if (K > h->last_rad) continue;
+                    const int m1 = k1 / a.Lx_factor, m2 = k2 / a.Ly_factor, m3 = k3 / a.Lz_factor;
+                    const long long idx = ((long long)(m2 >= 0 ? m2 : m2 + g.Ky) * g.Kx + (m1 >= 0 ? m1 : m1 + g.Kx)) * g.Kz + m3;
+                    for (int ic = 0; ic <= 1; ic++) {
+                        const double ru = ((double)rand() / RAND_MAX) * 2.0 - 1.0;
+                        const double rv = ((double)rand() / RAND_MAX) * 2.0 - 1.0;
+                        const double rw = ((double)rand() / RAND_MAX) * 2.0 - 1.0;
+                        double *pu = &uvw[idx].x, *pv = &uvw[g.S0 + idx].x, *pw = &uvw[2 * g.S0 + idx].x;
+                        pu[ic] = ru; pv[ic] = rv; pw[ic] = rw;
+                    }
+                }
+            }
+        }
+    }
+}
+
+// Input_Real_Field (src/HIT_LES.cpp:542-599, 738-763, 1268-1294): forward DFT of
+// the file box on the GPU (direct sums, init only), normalisation, file energy
+// and enstrophy, truncation to the retained modes.
+static int file_init(spns_handle *h, const double *file_uvw, std::vector<double2> &uvw) {
+    const spns_hit_args &a = h->a;
+    const Geo &g = h->g;
+    const int nx = actual_n(a.Nx_file, a.Lx_factor), ny = actual_n(a.Ny_file, a.Ly_factor), nz = actual_n(a.Nz_file, a.Lz_factor);
+    const int hzf = nz / 2 + 1;
+    const long long nf = (long long)nx * ny * nz;
+    const long long nspec = (long long)nx * ny * hzf;
+    uvw.assign(3 * (size_t)g.S0, make_double2(0.0, 0.0));
+    h->Ek_init_file = 0.0;
+    h->Enstrophy_init_file = 0.0;
+    double2 *d_in = nullptr, *d_a = nullptr, *d_b = nullptr;
+    int *d_k = nullptr;
+    double2 *twx = nullptr, *twy = nullptr, *twz = nullptr;
+    std::vector<double2> host_in(nf), spec(3 * (size_t)nspec);
+    CK(cudaMalloc(&d_in, sizeof(double2) * nf));
+    CK(cudaMalloc(&d_a, sizeof(double2) * nspec));
+    CK(cudaMalloc(&d_b, sizeof(double2) * nspec));
+    int maxn = std::max(nx, std::max(ny, nz));
+    CK(cudaMalloc(&d_k, sizeof(int) * maxn));
+    twx = make_twiddles(nx); twy = make_twiddles(ny); twz = make_twiddles(nz);
+    if (!twx || !twy || !twz) return fail(h, SPNS_ERR_OUT_OF_MEMORY, "twiddle allocation failed");
+    std::vector<int> kk(maxn);
+    for (int i = 0; i < maxn; i++) kk[i] = i;
+    CK(cudaMemcpy(d_k, kk.data(), sizeof(int) * maxn, cudaMemcpyHostToDevice));
+    for (int c = 0; c < 3; c++) {
+        for (long long i = 0; i < nf; i++) host_in[i] = make_double2(file_uvw[c * nf + i], 0.0);
+        CK(cudaMemcpy(d_in, host_in.data(), sizeof(double2) * nf, cudaMemcpyHostToDevice));
+        const int blocks = 148 * 16;
+        // z: lines (x,y), element stride 1 -> A[x][y][k3]
+        k_dft_axis<<<blocks, 256>>>(d_in, d_a, nz, hzf, d_k, (long long)nx * ny, 1, nz, hzf, 1, 1, twz);
+        CKL();
+        // y: lines (x,k3): in A[x][y][k3] stride hzf; out B[x][ky][k3]
+        k_dft_axis<<<blocks, 256>>>(d_a, d_b, ny, ny, d_k, (long long)nx * hzf, hzf, (long long)ny * hzf, (long long)ny * hzf, hzf, hzf, twy);
+        CKL();
+        // x: lines (ky,k3): stride ny*hzf; out C[kx][ky][k3]
+        k_dft_axis<<<blocks, 256>>>(d_b, d_a, nx, nx, d_k, (long long)ny * hzf, (long long)ny * hzf, 0, 0, (long long)ny * hzf,
+                                    (long long)ny * hzf, twx);
+        CKL();
+        CK(cudaMemcpy(spec.data() + c * nspec, d_a, sizeof(double2) * nspec, cudaMemcpyDeviceToHost));
+    }
+    cudaFree(d_in); cudaFree(d_a); cudaFree(d_b); cudaFree(d_k); cudaFree(twx); cudaFree(twy); cudaFree(twz);
+    const double normf = (double)nf;
+    for (auto &z : spec) { z.x /= normf; z.y /= normf; }
+    // Calculate_Ek_init_file over every file mode (expanded wavenumbers k = L*m)
+    for (int ia = 0; ia < nx; ia++)
+        for (int ib = 0; ib < ny; ib++)
+            for (int k3 = 0; k3 < hzf; k3++) {
+                const long long ind = ((long long)ia * ny + ib) * hzf + k3;
+                const long long k1 = (long long)a.Lx_factor * (ia <= nx / 2 ? ia : ia - nx);
+                const long long k2 = (long long)a.Ly_factor * (ib <= ny / 2 ? ib : ib - ny);
+                const long long kz3 = (long long)a.Lz_factor * k3;
+                const double rad2 = (double)(k1 * k1 + k2 * k2 + kz3 * kz3);
+                const bool conj = (k3 != 0) && !((nz % 2 == 0) && (k3 == nz / 2));
+                double E = 0.0;
+                for (int c = 0; c < 3; c++) E += spec[c * nspec + ind].x * spec[c * nspec + ind].x + spec[c * nspec + ind].y * spec[c * nspec + ind].y;
+                E *= 0.5;
+                if (conj) { h->Ek_init_file += 2 * E; h->Enstrophy_init_file += 2 * (2 * rad2 * E); }
+                else { h->Ek_init_file += E; h->Enstrophy_init_file += 2 * rad2 * E; }
+            }
+    // Truncate_Input_File_Fourier_Coefficients: |k_i| <= (N_file-1)/2 (expanded units)
+    for (int iy = 0; iy < g.Ky; iy++) {
+        const int m2 = iy <= g.hy ? iy : iy - g.Ky;
+        for (int ix = 0; ix < g.Kx; ix++) {
+            const int m1 = ix <= g.hx ? ix : ix - g.Kx;
+            for (int kz = 0; kz < g.Kz; kz++) {
+                const long long k1 = (long long)a.Lx_factor * m1, k2 = (long long)a.Ly_factor * m2, k3 = (long long)a.Lz_factor * kz;
+                if (std::llabs(k1) <= (a.Nx_file - 1) / 2 && std::llabs(k2) <= (a.Ny_file - 1) / 2 && k3 <= (a.Nz_file - 1) / 2) {
+                    const int fa = m1 >= 0 ? m1 : nx + m1, fb = m2 >= 0 ? m2 : ny + m2;
+                    if (fa < 0 || fa >= nx || fb < 0 || fb >= ny || kz >= hzf) continue;
+                    const long long ind = ((long long)fa * ny + fb) * hzf + kz;
+                    const long long ci = ((long long)iy * g.Kx + ix) * g.Kz + kz;
+                    for (int c = 0; c < 3; c++) uvw[c * g.S0 + ci] = spec[c * nspec + ind];
+                }
+            }
+        }
+    }
+    return SPNS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Helpers for API calls
+// ---------------------------------------------------------------------------
+static int forcing_energy_cascade(spns_handle *h, const double *Forced, int last_input_rad, int nullify) {
+    int r = shell_sums(h, 0, 0, 0);
+    if (r) return r;
+    const int nb = h->last_rad_max + 1;
+    k_totals<<<1, 1, 0, h->st>>>(h->bins, h->bins + nb, h->last_rad_max, h->ds, 0, 0.0);
+    CKL();
+    const int last_eff = std::min(last_input_rad, h->last_rad);
+    if (last_eff + 1 > h->forced_cap) {
+        if (h->forced) cudaFree(h->forced);
+        if (h->FT) cudaFree(h->FT);
+        h->forced = nullptr; h->FT = nullptr;
+        CK(cudaMalloc(&h->forced, sizeof(double) * (last_eff + 1)));
+        CK(cudaMalloc(&h->FT, sizeof(double) * (last_eff + 1)));
+        h->forced_cap = last_eff + 1;
+    }
+    CK(cudaMemcpyAsync(h->forced, Forced, sizeof(double) * (last_eff + 1), cudaMemcpyHostToDevice, h->st));
+    k_forcing_factors<<<1, 256, 0, h->st>>>(h->bins, h->forced, last_eff, h->FT);
+    CKL();
+    const long long n = h->g.S0;
+    int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 16);
+    k_forcing_scale<T64><<<blocks, 256, 0, h->st>>>(h->g, (cx<T64> *)h->U, (cx<T64> *)(h->U + n), (cx<T64> *)(h->U + 2 * n), h->FT,
+                                                    last_eff, nullify);
+    CKL();
+    if (h->a.isComplexConjugateCorrected) {
+        k_conj_correction<T64><<<64, 256, 0, h->st>>>(h->g, (cx<T64> *)h->U, (cx<T64> *)(h->U + n), (cx<T64> *)(h->U + 2 * n));
+        CKL();
+    }
+    // The forced state must be visible before the caller frees Forced.
+    CK(cudaStreamSynchronize(h->st));
+    return SPNS_OK;
+}
+
+static int totals(spns_handle *h, int what, double relambda) {
+    int r = shell_sums(h, 0, 0, 0);
+    if (r) return r;
+    const int nb = h->last_rad_max + 1;
+    k_totals<<<1, 1, 0, h->st>>>(h->bins, h->bins + nb, h->last_rad_max, h->ds, what, relambda);
+    CKL();
+    return SPNS_OK;
+}
+
+static int read_scalars(spns_handle *h, DevScalars *s) {
+    CK(cudaMemcpyAsync(s, h->ds, sizeof(*s), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return SPNS_OK;
+}
+
+static void free_handle(spns_handle *h) {
+    if (!h) return;
+    cudaFree(h->ds); cudaFree(h->U); cudaFree(h->R); cudaFree(h->Up); cudaFree(h->B1); cudaFree(h->B2);
+    cudaFree(h->bins); cudaFree(h->FT); cudaFree(h->forced); cudaFree(h->phys);
+    for (auto &kv : h->tw) cudaFree(kv.second);
+    for (auto ev : h->prof_ev) cudaEventDestroy(ev);
+    if (h->st) cudaStreamDestroy(h->st);
+    delete h;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char *spns_status_string(int s) {
+    switch (s) {
+    case SPNS_OK: return "ok";
+    case SPNS_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case SPNS_ERR_UNSUPPORTED_SIZE: return "unsupported size";
+    case SPNS_ERR_CUDA: return "CUDA error";
+    case SPNS_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case SPNS_ERR_NONFINITE: return "non-finite value";
+    case SPNS_ERR_DOMAIN: return "time-step angle out of range";
+    default: return "unknown status";
+    }
+}
+
+const char *spns_last_error(spns_handle *h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+int spns_create(const spns_hit_args *args, const double *file_uvw, spns_handle **out) {
+    spns_handle *h = nullptr;
+    if (!args || !out) return fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    if (args->precision != SPNS_FP64) return fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "precision %d not available in this build", args->precision);
+    if (args->Lx_factor < 1 || args->Ly_factor < 1 || args->Lz_factor < 1 || args->Nx < 2 || args->Ny < 2 || args->Nz < 2)
+        return fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "invalid sizes or length factors");
+    if (args->isInitialFieldFromFile && !file_uvw) return fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "file initial field requested without data");
+    h = new spns_handle();
+    h->a = *args;
+    const spns_hit_args &a = h->a;
+    int rc;
+    {
+        cudaError_t e = cudaSetDevice(a.device);
+        if (e != cudaSuccess) { fail(nullptr, SPNS_ERR_CUDA, "cudaSetDevice(%d): %s", a.device, cudaGetErrorString(e)); delete h; return SPNS_ERR_CUDA; }
+    }
+    // geometry (true grid of a non-cubic box, src/HIT_LES.h:31-36)
+    Geo &g = h->g;
+    const int ANx = actual_n(a.Nx, a.Lx_factor), ANy = actual_n(a.Ny, a.Ly_factor), ANz = actual_n(a.Nz, a.Lz_factor);
+    const int AMx = actual_n(a.Mx, a.Lx_factor), AMy = actual_n(a.My, a.Ly_factor), AMz = actual_n(a.Mz, a.Lz_factor);
+    g.hx = ANx / 2; g.hy = ANy / 2; g.hz = ANz / 2;
+    g.Kx = 2 * g.hx + 1; g.Ky = 2 * g.hy + 1; g.Kz = g.hz + 1;
+    g.Mx = AMx; g.My = AMy; g.Mz = AMz;
+    g.sx = a.Lx_factor; g.sy = a.Ly_factor; g.sz = a.Lz_factor;
+    g.S0 = (long long)g.Ky * g.Kx * g.Kz;
+    g.S1 = (long long)g.Ky * g.Mx * g.Kz;
+    g.S2 = (long long)g.My * g.Mx * g.Kz;
+    if (!length_supported(g.Mx) || !length_supported(g.My) || !length_supported(g.Mz)) {
+        rc = fail(nullptr, SPNS_ERR_UNSUPPORTED_SIZE, "FFT grid %dx%dx%d outside the compiled lengths", g.Mx, g.My, g.Mz);
+        delete h; return rc;
+    }
+    if (2 * g.hx >= g.Mx || 2 * g.hy >= g.My || 2 * g.hz >= g.Mz) {
+        rc = fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "retained modes do not fit the FFT grid");
+        delete h; return rc;
+    }
+    h->last_rad = std::min((a.Nx - 1) / 2, std::min((a.Ny - 1) / 2, (a.Nz - 1) / 2));
+    h->last_rad_max = (int)std::ceil(std::sqrt(1.0 * (a.Nx / 2) * (a.Nx / 2) + 1.0 * (a.Ny / 2) * (a.Ny / 2) + 1.0 * (a.Nz / 2) * (a.Nz / 2)));
+    const double PI_ = 3.141592653589793238462643;
+    StepConsts &c = h->c;
+    memset(&c, 0, sizeof(c));
+    c.inv_norm = 1.0 / ((double)g.Mx * g.My * g.Mz);
+    c.omega_x = a.omega_x; c.omega_y = a.omega_y; c.omega_z = a.omega_z;
+    c.Ax = 2.0 * PI_ / AMx / a.Lx_factor; c.Ay = 2.0 * PI_ / AMy / a.Ly_factor; c.Az = 2.0 * PI_ / AMz / a.Lz_factor;
+    c.inv_Ax = 1.0 / c.Ax; c.inv_Ay = 1.0 / c.Ay; c.inv_Az = 1.0 / c.Az;
+    c.C_At = a.C_At;
+    h->delta = 2.0 * PI_ / std::cbrt((double)((long long)a.Lx_factor * a.Ly_factor * a.Lz_factor * AMx * AMy * AMz));
+    c.les_ct = a.C_Smag * a.C_Smag * h->delta * h->delta;
+    c.fixed_dt = a.fixed_dt;
+    c.eps_on = a.eps_forcing > 0.0;
+    c.eps_kmin = a.eps_kmin; c.eps_kmax = a.eps_kmax;
+    c.rotating = a.isRotating;
+    c.self_adaptive = a.isSelfAdaptive;
+    // self-adaptive constants (src/HIT_LES.cpp:1049-1078)
+    c.Ah = (c.Ax + c.Ay + c.Az) / 3.0;
+    c.t1 = 0.9302468;
+    c.kopt_k[0] = 0.73782212; c.kopt_k[1] = 0.44660387;
+    c.phi[0] = std::atan(164.0 / 99.0); c.phi[1] = PI_ / 3.0; c.phi[2] = PI_ * 3.0 * 3.0 / (5.0 * 5.0);
+    const double cc[14] = {0.0647998, -0.386022, 3.72945, -9.38143, 7.06574, 2403400.0, -5018490.0,
+                           2620140.0, 2945.0, -6665.76, 3790.54, 4.80513, -16.9473, 15.0155};
+    memcpy(c.c, cc, sizeof(cc));
+
+    // device memory
+    auto cleanup = [&](int code) { free_handle(h); return code; };
+    if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) return cleanup(fail(nullptr, SPNS_ERR_CUDA, "stream creation failed"));
+    const bool rot = !a.isLES && a.nonlinear_form == 1;
+    h->nB1 = rot ? 5 : 6;
+    h->nB2 = rot ? 6 : 9;
+    size_t s0 = sizeof(double2) * 3 * g.S0;
+    bool okm = cudaMalloc(&h->ds, sizeof(DevScalars)) == cudaSuccess && cudaMalloc(&h->U, s0) == cudaSuccess &&
+               cudaMalloc(&h->R, s0) == cudaSuccess &&
+               (!a.isSelfAdaptive || cudaMalloc(&h->Up, s0) == cudaSuccess) &&
+               cudaMalloc(&h->B1, sizeof(double2) * h->nB1 * g.S1) == cudaSuccess &&
+               cudaMalloc(&h->B2, sizeof(double2) * h->nB2 * g.S2) == cudaSuccess &&
+               cudaMalloc(&h->bins, sizeof(double) * 2 * (h->last_rad_max + 1)) == cudaSuccess;
+    if (!okm) { cudaGetLastError(); return cleanup(fail(nullptr, SPNS_ERR_OUT_OF_MEMORY, "device allocation failed")); }
+    for (int L : {g.Mx, g.My, g.Mz})
+        if (!h->tw.count(L)) {
+            double2 *t = make_twiddles(L);
+            if (!t) return cleanup(fail(nullptr, SPNS_ERR_OUT_OF_MEMORY, "twiddle allocation failed"));
+            h->tw[L] = t;
+        }
+    cudaMemset(h->R, 0, s0);
+    if (h->Up) cudaMemset(h->Up, 0, s0);
+    DevScalars s0v;
+    memset(&s0v, 0, sizeof(s0v));
+    s0v.nu = a.nu;
+    s0v.kappa = 0.5;
+    if (cudaMemcpy(h->ds, &s0v, sizeof(s0v), cudaMemcpyHostToDevice) != cudaSuccess)
+        return cleanup(fail(nullptr, SPNS_ERR_CUDA, "scalar upload failed"));
+
+    // initial field
+    std::vector<double2> uvw;
+    if (a.isInitialFieldFromFile) {
+        rc = file_init(h, file_uvw, uvw);
+        if (rc) { g_create_error = h->err; return cleanup(rc); }
+        if (cudaMemcpy(h->U, uvw.data(), s0, cudaMemcpyHostToDevice) != cudaSuccess)
+            return cleanup(fail(nullptr, SPNS_ERR_CUDA, "state upload failed"));
+    } else {
+        k41_host(h, uvw);
+        if (cudaMemcpy(h->U, uvw.data(), s0, cudaMemcpyHostToDevice) != cudaSuccess)
+            return cleanup(fail(nullptr, SPNS_ERR_CUDA, "state upload failed"));
+        const long long n = g.S0;
+        k_conj_correction<T64><<<64, 256, 0, h->st>>>(g, (cx<T64> *)h->U, (cx<T64> *)(h->U + n), (cx<T64> *)(h->U + 2 * n));
+        std::vector<double> K41((size_t)h->last_rad + 1, 0.0);
+        for (int K = 1; K <= h->last_rad; K++) K41[K] = std::pow((double)K, -5.0 / 3.0);
+        rc = forcing_energy_cascade(h, K41.data(), h->last_rad, 0);
+        if (rc) { g_create_error = h->err; return cleanup(rc); }
+    }
+    rc = run_velocity(h, nullptr);
+    if (rc) { g_create_error = h->err; return cleanup(rc); }
+    if (!a.isReLambda) {
+        k_recalc_dt<<<1, 1, 0, h->st>>>(h->c, h->ds);
+    }
+    rc = totals(h, 0, 0.0);
+    if (rc) { g_create_error = h->err; return cleanup(rc); }
+    DevScalars sv;
+    rc = read_scalars(h, &sv);
+    if (rc) { g_create_error = h->err; return cleanup(rc); }
+    h->Ek_init = sv.ek_tot;
+    *out = h;
+    return SPNS_OK;
+}
+
+int spns_destroy(spns_handle *h) {
+    if (!h) return SPNS_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(h->a.device);
+    cudaStreamSynchronize(h->st);
+    free_handle(h);
+    return SPNS_OK;
+}
+
+int spns_step(spns_handle *h, int nsteps) {
+    if (!h || nsteps < 0) return SPNS_ERR_INVALID_ARGUMENT;
+    for (int i = 0; i < nsteps; i++) {
+        int r = step_once(h);
+        if (r) return r;
+    }
+    return check_flags(h);
+}
+
+int spns_recalculate_timestep(spns_handle *h) {
+    if (!h) return SPNS_ERR_INVALID_ARGUMENT;
+    k_recalc_dt<<<1, 1, 0, h->st>>>(h->c, h->ds);
+    CKL();
+    return SPNS_OK;
+}
+
+int spns_forcing_energy_cascade(spns_handle *h, const double *Forced_Ek, int last_input_rad, int nullify) {
+    if (!h || !Forced_Ek || last_input_rad < 0) return SPNS_ERR_INVALID_ARGUMENT;
+    return forcing_energy_cascade(h, Forced_Ek, last_input_rad, nullify);
+}
+
+int spns_forcing_reynolds_lambda(spns_handle *h, double relambda) {
+    if (!h) return SPNS_ERR_INVALID_ARGUMENT;
+    return totals(h, 2, relambda);
+}
+
+int spns_recalculate_reynolds_lambda(spns_handle *h, double *relambda) {
+    if (!h) return SPNS_ERR_INVALID_ARGUMENT;
+    int r = totals(h, 1, 0.0);
+    if (r) return r;
+    if (relambda) {
+        DevScalars s;
+        r = read_scalars(h, &s);
+        if (r) return r;
+        *relambda = s.relambda;
+    }
+    return SPNS_OK;
+}
+
+int spns_recalculate_energy(spns_handle *h, double *ek) {
+    if (!h) return SPNS_ERR_INVALID_ARGUMENT;
+    int r = totals(h, 0, 0.0);
+    if (r) return r;
+    if (ek) { DevScalars s; r = read_scalars(h, &s); if (r) return r; *ek = s.ek_tot; }
+    return SPNS_OK;
+}
+
+int spns_recalculate_enstrophy(spns_handle *h, double *ok) {
+    if (!h) return SPNS_ERR_INVALID_ARGUMENT;
+    int r = totals(h, 3, 0.0);
+    if (r) return r;
+    if (ok) { DevScalars s; r = read_scalars(h, &s); if (r) return r; *ok = s.ok_tot; }
+    return SPNS_OK;
+}
+
+int spns_recalculate_energy_cascade(spns_handle *h, double *Ek, double *ek_tot) {
+    if (!h) return SPNS_ERR_INVALID_ARGUMENT;
+    int r = totals(h, 0, 0.0);
+    if (r) return r;
+    if (Ek) { CK(cudaMemcpyAsync(Ek, h->bins, sizeof(double) * (h->last_rad_max + 1), cudaMemcpyDeviceToHost, h->st)); }
+    DevScalars s;
+    r = read_scalars(h, &s);
+    if (r) return r;
+    if (ek_tot) *ek_tot = s.ek_tot;
+    return SPNS_OK;
+}
+
+int spns_velocity_antitransform(spns_handle *h) {
+    if (!h) return SPNS_ERR_INVALID_ARGUMENT;
+    return run_velocity(h, nullptr);
+}
+
+int spns_complex_conjugate_correction(spns_handle *h) {
+    if (!h) return SPNS_ERR_INVALID_ARGUMENT;
+    const long long n = h->g.S0;
+    k_conj_correction<T64><<<64, 256, 0, h->st>>>(h->g, (cx<T64> *)h->U, (cx<T64> *)(h->U + n), (cx<T64> *)(h->U + 2 * n));
+    CKL();
+    return SPNS_OK;
+}
+
+int spns_check_physfour_energy(spns_handle *h, double atol, int *ok, double *d1, double *d2) {
+    if (!h) return SPNS_ERR_INVALID_ARGUMENT;
+    int r = totals(h, 0, 0.0);
+    if (r) return r;
+    DevScalars s;
+    r = read_scalars(h, &s);
+    if (r) return r;
+    const double EkFour = s.ek_tot;
+    r = run_velocity(h, nullptr);
+    if (r) return r;
+    r = read_scalars(h, &s);
+    if (r) return r;
+    const double EkReal = 0.5 * s.sumsq_phys / ((double)h->g.Mx * h->g.My * h->g.Mz);
+    const double diff1 = std::fabs(EkReal - EkFour), diff2 = 0.0; // EkSpNS is the same shell integral as EkFour here
+    if (d1) *d1 = diff1;
+    if (d2) *d2 = diff2;
+    if (ok) *ok = (diff1 <= atol && diff2 <= atol);
+    return SPNS_OK;
+}
+
+int spns_get_scalars(spns_handle *h, spns_scalars *o) {
+    if (!h || !o) return SPNS_ERR_INVALID_ARGUMENT;
+    DevScalars s;
+    int r = read_scalars(h, &s);
+    if (r) return r;
+    o->time = s.time; o->At = s.dt; o->nu = s.nu; o->Ek_Tot = s.ek_tot; o->Ok_Tot = s.ok_tot; o->ReLambda = s.relambda;
+    o->Ek_init = h->Ek_init; o->Ek_init_file = h->Ek_init_file; o->Enstrophy_init_file = h->Enstrophy_init_file;
+    o->kappa = s.kappa; o->MaxVel = s.maxvel; o->iter = s.iter; o->last_rad = h->last_rad; o->last_rad_max = h->last_rad_max;
+    return SPNS_OK;
+}
+
+int spns_set_nu(spns_handle *h, double nu) {
+    if (!h) return SPNS_ERR_INVALID_ARGUMENT;
+    CK(cudaMemcpyAsync((char *)h->ds + offsetof(DevScalars, nu), &nu, sizeof(double), cudaMemcpyHostToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return SPNS_OK;
+}
+
+int spns_spectral_dims(spns_handle *h, int *Kx, int *Ky, int *Kz) {
+    if (!h) return SPNS_ERR_INVALID_ARGUMENT;
+    if (Kx) *Kx = h->g.Kx;
+    if (Ky) *Ky = h->g.Ky;
+    if (Kz) *Kz = h->g.Kz;
+    return SPNS_OK;
+}
+
+int spns_physical_dims(spns_handle *h, int *Mx, int *My, int *Mz) {
+    if (!h) return SPNS_ERR_INVALID_ARGUMENT;
+    if (Mx) *Mx = h->g.Mx;
+    if (My) *My = h->g.My;
+    if (Mz) *Mz = h->g.Mz;
+    return SPNS_OK;
+}
+
+int spns_get_spectral(spns_handle *h, double *uvw) {
+    if (!h || !uvw) return SPNS_ERR_INVALID_ARGUMENT;
+    CK(cudaMemcpyAsync(uvw, h->U, sizeof(double2) * 3 * h->g.S0, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return SPNS_OK;
+}
+
+int spns_set_spectral(spns_handle *h, const double *uvw) {
+    if (!h || !uvw) return SPNS_ERR_INVALID_ARGUMENT;
+    CK(cudaMemcpyAsync(h->U, uvw, sizeof(double2) * 3 * h->g.S0, cudaMemcpyHostToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return SPNS_OK;
+}
+
+int spns_get_physical(spns_handle *h, double *uvw) {
+    if (!h || !uvw) return SPNS_ERR_INVALID_ARGUMENT;
+    const long long n3 = (long long)h->g.Mx * h->g.My * h->g.Mz;
+    if (!h->phys) CK(cudaMalloc(&h->phys, sizeof(double) * 3 * n3));
+    int r = run_velocity(h, h->phys);
+    if (r) return r;
+    CK(cudaMemcpyAsync(uvw, h->phys, sizeof(double) * 3 * n3, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return SPNS_OK;
+}
+
+int spns_device_state(spns_handle *h, void **u, void **v, void **w) {
+    if (!h) return SPNS_ERR_INVALID_ARGUMENT;
+    if (u) *u = h->U;
+    if (v) *v = h->U + h->g.S0;
+    if (w) *w = h->U + 2 * h->g.S0;
+    return SPNS_OK;
+}
+
+int spns_stream(spns_handle *h, void **stream) {
+    if (!h || !stream) return SPNS_ERR_INVALID_ARGUMENT;
+    *stream = (void *)h->st;
+    return SPNS_OK;
+}
+
+int spns_kernels_per_step(spns_handle *h, int *count) {
+    if (!h || !count) return SPNS_ERR_INVALID_ARGUMENT;
+    *count = h->kernels_per_step;
+    return SPNS_OK;
+}
+
+int spns_profile_begin(spns_handle *h, int max_steps) {
+    if (!h || max_steps < 0) return SPNS_ERR_INVALID_ARGUMENT;
+    for (auto ev : h->prof_ev) cudaEventDestroy(ev);
+    h->prof_ev.clear();
+    h->prof_names.clear();
+    h->prof_steps = 0;
+    h->prof_nk = 0;
+    h->prof_cap_steps = 0;
+    const int per = 16; // upper bound of kernels per step + 1
+    h->prof_ev.resize((size_t)max_steps * per);
+    for (auto &ev : h->prof_ev) CK(cudaEventCreate(&ev));
+    h->prof_cap_steps = max_steps;
+    return SPNS_OK;
+}
+
+int spns_profile_read(spns_handle *h, float *ms, int cap, int *nkernels, int *nsteps) {
+    if (!h) return SPNS_ERR_INVALID_ARGUMENT;
+    CK(cudaStreamSynchronize(h->st));
+    const int nk = h->prof_nk, per = nk + 1;
+    if (nkernels) *nkernels = nk;
+    if (nsteps) *nsteps = h->prof_steps;
+    for (int s = 0; s < h->prof_steps; s++)
+        for (int k = 0; k < nk; k++) {
+            const int i = s * nk + k;
+            if (!ms || i >= cap) continue;
+            // events of step s live in a block of 16 slots
+            CK(cudaEventElapsedTime(&ms[i], h->prof_ev[(size_t)s * 16 + k], h->prof_ev[(size_t)s * 16 + k + 1]));
+        }
+    (void)per;
+    h->prof_cap_steps = 0;
+    return SPNS_OK;
+}
+
+const char *spns_profile_kernel_name(spns_handle *h, int i) {
+    if (!h || i < 0 || i >= (int)h->prof_names.size()) return "";
+    return h->prof_names[i].c_str();
+}
+
+} // extern "C"
+
+// ---------------------------------------------------------------------------
+// Test building block: batched 1-D FFT of contiguous lines (one line per
+// pencil, pencil-major shared-memory layout as in the z pass).
+// ---------------------------------------------------------------------------
+template <int L>
+__global__ void k_fft1d_lines(double2 *data, int batch, int sign, const double2 *tw) {
+    using S = Shape<double, L>;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    constexpr int E = S::E, Q = S::Q, P = S::P;
+    const int tid = threadIdx.x, p = tid / Q, q = tid % Q;
+    const long long line = (long long)blockIdx.x * P + p;
+    const bool ok = line < batch;
+    cx<double> *d = reinterpret_cast<cx<double> *>(data) + (ok ? line : 0) * L;
+    SmPencil<double, L> sm{reinterpret_cast<cx<double> *>(smraw) + p * SmPencil<double, L>::PITCH};
+    cx<double> r[E];
+    if (sign < 0) {
+#pragma unroll
+        for (int e = 0; e < E; e++) r[e] = ok ? d[in_row<L, E, false>(q, e)] : zero<double>();
+        fft<double, L, E, false>(r, sm, q, (const cx<double> *)tw);
+        if (ok)
+#pragma unroll
+            for (int e = 0; e < E; e++) d[out_row<L, E, false>(q, e)] = r[e];
+    } else {
+#pragma unroll
+        for (int e = 0; e < E; e++) r[e] = ok ? d[in_row<L, E, true>(q, e)] : zero<double>();
+        fft<double, L, E, true>(r, sm, q, (const cx<double> *)tw);
+        if (ok)
+#pragma unroll
+            for (int e = 0; e < E; e++) d[out_row<L, E, true>(q, e)] = r[e];
+    }
+}
+
+extern "C" int spns_fft1d_batch_f64(void *data_dev, int n, int batch, int sign) {
+    spns_handle *h = nullptr;
+    if (!data_dev || batch < 0 || (sign != 1 && sign != -1)) return fail(h, SPNS_ERR_INVALID_ARGUMENT, "invalid argument");
+    if (!length_supported(n)) return fail(h, SPNS_ERR_UNSUPPORTED_SIZE, "FFT length %d is not compiled", n);
+    static std::map<std::pair<int, int>, double2 *> tws;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    auto key = std::make_pair(dev, n);
+    if (!tws.count(key)) {
+        double2 *t = make_twiddles(n);
+        if (!t) return fail(h, SPNS_ERR_OUT_OF_MEMORY, "twiddle allocation failed");
+        tws[key] = t;
+    }
+    const double2 *tw = tws[key];
+#define SPNS_FFT1D(LL)                                                                            \
+    if (n == LL) {                                                                                \
+        using S = Shape<double, LL>;                                                              \
+        auto kern = k_fft1d_lines<LL>;                                                            \
+        if (set_smem(kern, S::SMEM_PEN) != cudaSuccess) return fail(h, SPNS_ERR_CUDA, "smem attribute"); \
+        if (batch > 0) kern<<<(batch + S::P - 1) / S::P, S::THREADS, S::SMEM_PEN>>>((double2 *)data_dev, batch, sign, tw); \
+    }
+    SPNS_FOR_EACH_LENGTH(SPNS_FFT1D)
+#undef SPNS_FFT1D
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return fail(h, SPNS_ERR_CUDA, "fft1d: %s", cudaGetErrorString(e));
+    return SPNS_OK;
+}
