@@ -53,18 +53,24 @@ def box_args(N: int, self_adaptive: bool = True):
                    isRotating=False, isLES=False, isComplexConjugateCorrected=False, isSelfAdaptive=self_adaptive)
 
 
-def algorithmic_bytes(N: int, self_adaptive: bool = True, word: int = 16):
-    """Bytes each kernel must move once (arrays read + written, each counted once)."""
+def algorithmic_bytes(N: int, self_adaptive: bool = True, word: int = 16, form: str = "advective"):
+    """Bytes each kernel must move once (arrays read + written, each counted once).
+
+    S0 = compact spectral field, S1 = after the x transform, S2 = after the y
+    transform (complex elements of `word` bytes).  Advective form: K1 3 S0 -> 6 S1,
+    K2 6 S1 -> 9 S2, K3 9 S2 -> 3 S2, K4 3 S2 -> 3 S1, K5 3 S1 -> 3 S0 (nonlinear
+    term G), K6 reads G, u, R^{n-1} (+ u^{n-1}) and writes R^n, u^{n+1}."""
     h = N // 2
     K, M, Kz = 2 * h + 1, (3 * N) // 2, h + 1
     S0, S1, S2 = K * K * Kz, K * M * Kz, M * M * Kz
-    k5_state = (18 if self_adaptive else 12) * S0
+    n1, n2 = (6, 9) if form == "advective" else (5, 6)
     return {
-        "k1_inv_x": (3 * S0 + 5 * S1) * word,
-        "k2_inv_y": (5 * S1 + 6 * S2) * word,
-        "k3_z": (6 * S2 + 3 * S2) * word,
+        "k1_inv_x": (3 * S0 + n1 * S1) * word,
+        "k2_inv_y": (n1 * S1 + n2 * S2) * word,
+        "k3_z": (n2 * S2 + 3 * S2) * word,
         "k4_fwd_y": (3 * S2 + 3 * S1) * word,
-        "k5_fwd_x_sweep": (3 * S1 + k5_state) * word,
+        "k5_fwd_x": (3 * S1 + 3 * S0) * word,
+        "k6_sweep": ((18 if self_adaptive else 15) * S0) * word,
         "shell_sums": 3 * S0 * word,
     }, dict(S0=S0, S1=S1, S2=S2)
 
@@ -298,6 +304,7 @@ def run_gpu(args):
     if os.path.exists(tp):
         with open(tp) as fh:
             traffic = json.load(fh).get(dom)
+    step_bytes = sum(v for k, v in bytes_per.items() if k != "shell_sums") + bytes_per["shell_sums"]
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -307,7 +314,8 @@ def run_gpu(args):
                                "self-adaptive dt C_At=0.5, FP64 plain form",
                    "N": N, "fft_grid": (3 * N) // 2, "parallelism": f"replicas x{world}",
                    "l2": f"inputs larger than L2 (state {3 * sizes['S0'] * 16 / 1e9:.1f} GB, work buffers "
-                         f"{(5 * sizes['S1'] + 6 * sizes['S2']) * 16 / 1e9:.1f} GB)",
+                         f"{(6 * sizes['S1'] + 9 * sizes['S2']) * 16 / 1e9:.1f} GB)",
+                   "nonlinear_form": "advective (u.grad u, as the reference)",
                    "finite": finite},
         "clocks": clk.summary(),
         "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": 0,
@@ -315,6 +323,8 @@ def run_gpu(args):
                 "loop": "HIT.New_Fractional_Step_Method() + Recalculate_Energy_Cascade() (E(K) to host) per step"},
         "gpu_launches": nk * args.steps,
         "kernel_ms": share,
+        "step_algorithmic_bytes": step_bytes,
+        "step_achieved_GBps": step_bytes / (ms_max / args.steps / 1e3) / 1e9,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                      "algorithmic_bytes": bytes_per[dom]},

@@ -166,9 +166,14 @@ template <int L, int E, bool INV> __device__ __forceinline__ int out_row(int q, 
     return q + PL::Q * (e / R) + (e % R) * (L / R);
 }
 
+// The thread index goes through an opaque move so that the shared-memory
+// addresses of the stages are recomputed per transform instead of being kept
+// live across every transform of a kernel (which exhausts the register file).
 template <typename T, int L, int E, bool INV, class SM>
 __device__ __forceinline__ void fft(cx<T> (&v)[E], SM sm, int q, const cx<T> *__restrict__ tw) {
-    fft_run<T, L, E, INV, 0, SM>(v, sm, q, tw);
+    int qq;
+    asm volatile("mov.b32 %0, %1;" : "=r"(qq) : "r"(q));
+    fft_run<T, L, E, INV, 0, SM>(v, sm, qq, tw);
 }
 
 // Accessor: tile of P pencils stored row-major [row][P] (pencil index fastest).

@@ -11,16 +11,19 @@
 // box of the reference (src/MAIN.cpp:216-260, src/HIT_LES.cpp:867-871) runs on
 // its true grid (ActualM) instead of the expanded one.
 //
-// Pass plan of one step (DNS, rotational form of the nonlinear term):
-//   K1 inverse x : S0 u,v,w          -> S1 u,v,w, w_y=i(kz u-kx w), i kx v
-//   K2 inverse y : S1 (5)            -> S2 u,v,w, w_x, w_y, w_z
-//   K3 z         : c2r of 6 fields, c = w x u (+ CFL maxima), r2c -> S2 c_x,c_y,c_z
+// Pass plan of one step (DNS, advective form of the reference):
+//   K1 inverse x : S0 u,v,w          -> S1 u,v,w, du/dx, dv/dx, dw/dx
+//   K2 inverse y : S1 (6)            -> S2 + du/dy, dv/dy, dw/dy (9)
+//   K3 z         : c2r of 12 fields (dz from u,v,w), conv = u_j d_j u_i (+ CFL
+//                  maxima), r2c -> S2 conv_x, conv_y, conv_z
 //   K4 forward y : S2 (3)            -> S1 (3)
-//   K5 forward x : S1 (3)            -> S0 spectral sweep: 1/M^3, R, Coriolis,
-//                  forcing, AB2 or kappa-scheme predictor, projection.
-// LES (Smagorinsky) carries the 9 velocity gradients and folds the divergence of
-// the SGS stress into the forward passes (i kz tau_i3 in K3, i ky tau_i2 in K4,
-// i kx tau_i1 in K5).
+//   K5 forward x : S1 (3)            -> S0 G (3)
+//   K6 sweep     : G, u, R^{n-1} [, u^{n-1}] -> 1/M^3, R, Coriolis, forcing,
+//                  AB2 or kappa-scheme predictor, projection -> u^{n+1}, R^n.
+// The rotational form (opt-in) carries u and the vorticity instead (5, 6 and 6
+// fields in K1, K2, K3).  LES (Smagorinsky) adds the SGS stress, whose
+// divergence is folded into the forward passes (i kz t_i3 in K3, i ky t_i2 in
+// K4, i kx t_i1 in K5).
 #pragma once
 #include "fft_core.cuh"
 
@@ -74,7 +77,7 @@ template <int MODE> struct Fields {
 //   VEL: u,v,w   ROT: u,v,w, w_y=i(kz u-kx w), i kx v   ADV/LES: u,v,w, du/dx, dv/dx, dw/dx
 // ===========================================================================
 template <typename T, int L, int E, int P, int MODE>
-__global__ void __launch_bounds__(P *(L / E)) k1_inv_x(Geo g, const cx<T> *__restrict__ u, const cx<T> *__restrict__ v,
+__global__ void __launch_bounds__(P *(L / E), 2) k1_inv_x(Geo g, const cx<T> *__restrict__ u, const cx<T> *__restrict__ v,
                                                        const cx<T> *__restrict__ w, cx<T> *__restrict__ out,
                                                        const cx<T> *__restrict__ tw) {
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -123,7 +126,7 @@ __global__ void __launch_bounds__(P *(L / E)) k1_inv_x(Geo g, const cx<T> *__res
 //   ADV/LES: u,v,w, du/dx,dv/dx,dw/dx, du/dy,dv/dy,dw/dy
 // ===========================================================================
 template <typename T, int L, int E, int P, int MODE>
-__global__ void __launch_bounds__(P *(L / E)) k2_inv_y(Geo g, const cx<T> *__restrict__ in, cx<T> *__restrict__ out,
+__global__ void __launch_bounds__(P *(L / E), 2) k2_inv_y(Geo g, const cx<T> *__restrict__ in, cx<T> *__restrict__ out,
                                                        const cx<T> *__restrict__ tw) {
     extern __shared__ __align__(16) unsigned char smraw[];
     const int tid = threadIdx.x, p = tid % P, q = tid / P;
@@ -296,7 +299,8 @@ __device__ __forceinline__ void cfl_update(double (&mx)[4], double uu, double vv
 }
 
 // Shared-memory slots of physical fields kept per pencil (rows of this thread only).
-template <int MODE> struct K3Phys { static constexpr int N = MODE == MODE_ADV ? 3 : MODE == MODE_LES ? 9 : 0; };
+// slots: 0 u, 1 v, 2 w, 3..5 conv_x,y,z, LES 6..11 a11, a12, a22, a13, a23, a33 (then t_ij)
+template <int MODE> struct K3Phys { static constexpr int N = MODE == MODE_ADV ? 6 : MODE == MODE_LES ? 12 : 0; };
 
 template <typename T, int L, int E, int P, int MODE>
 __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ buf, StepConsts c, DevScalars *ds,
@@ -313,16 +317,15 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
     SmPencil<T, L> sm{smc + p * SmPencil<T, L>::PITCH};
     T *ph = reinterpret_cast<T *>(smc + P * SmPencil<T, L>::PITCH) + (long long)p * NPH * L;
     const T sz = T(g.sz);
-    cx<T> *F[9];
-#pragma unroll
-    for (int i = 0; i < 9; i++) F[i] = buf + (long long)i * g.S2 + base;
+    cx<T> *const B0 = buf + base;
+#define F(i) (B0 + (long long)(i) * g.S2)
     double mx[4] = {0.0, 0.0, 0.0, 0.0};
 
     if constexpr (MODE == MODE_VEL) {
         cx<T> A[E], B[E];
-        k3_load_pair<T, L, E>(A, F[0], false, F[1], false, g.Kz, sz, q, ok);
+        k3_load_pair<T, L, E>(A, F(0), false, F(1), false, g.Kz, sz, q, ok);
         fft<T, L, E, true>(A, sm, q, tw);
-        k3_load_pair<T, L, E>(B, F[2], false, nullptr, false, g.Kz, sz, q, ok);
+        k3_load_pair<T, L, E>(B, F(2), false, nullptr, false, g.Kz, sz, q, ok);
         fft<T, L, E, true>(B, sm, q, tw);
         double ss = 0.0;
 #pragma unroll
@@ -347,11 +350,11 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
     } else if constexpr (MODE == MODE_ROT) {
         // pairs (u, w_x), (v, w_y), (w, w_z);  c = w x u  (= u.grad u + gradient)
         cx<T> A[E], B[E], C[E];
-        k3_load_pair<T, L, E>(A, F[0], false, F[3], false, g.Kz, sz, q, ok);
+        k3_load_pair<T, L, E>(A, F(0), false, F(3), false, g.Kz, sz, q, ok);
         fft<T, L, E, true>(A, sm, q, tw);
-        k3_load_pair<T, L, E>(B, F[1], false, F[4], false, g.Kz, sz, q, ok);
+        k3_load_pair<T, L, E>(B, F(1), false, F(4), false, g.Kz, sz, q, ok);
         fft<T, L, E, true>(B, sm, q, tw);
-        k3_load_pair<T, L, E>(C, F[2], false, F[5], false, g.Kz, sz, q, ok);
+        k3_load_pair<T, L, E>(C, F(2), false, F(5), false, g.Kz, sz, q, ok);
         fft<T, L, E, true>(C, sm, q, tw);
 #pragma unroll
         for (int e = 0; e < E; e++) {
@@ -362,23 +365,23 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
         }
         if (!ok) { mx[0] = mx[1] = mx[2] = mx[3] = 0.0; }
         block_max4<T>(mx, ds);
-        k3_store_pair<T, L, E>(A, sm, q, g.Kz, F[0], F[1], false, sz, ok, tw);
-        k3_store_single<T, L, E>(B, sm, q, g.Kz, F[2], ok, tw);
+        k3_store_pair<T, L, E>(A, sm, q, g.Kz, F(0), F(1), false, sz, ok, tw);
+        k3_store_single<T, L, E>(B, sm, q, g.Kz, F(2), ok, tw);
     } else {
         // Advective form of the reference (src/HIT_LES.cpp:74-125): conv_i = u_j d_j u_i.
         // S2 inputs: 0 u, 1 v, 2 w, 3 du/dx, 4 dv/dx, 5 dw/dx, 6 du/dy, 7 dv/dy, 8 dw/dy;
-        // z-derivatives are formed here from u, v, w.
-        // LES (src/HIT_LES.cpp:130-171): strain combinations a_ij accumulate in shared memory.
-        T cxv[E], cyv[E], czv[E];
+        // z-derivatives are formed here from u, v, w.  Physical values of the
+        // thread's own rows are kept in per-thread shared-memory slots (no barrier needed).
+        // LES (src/HIT_LES.cpp:130-171): strain combinations a_ij accumulate in further slots.
         cx<T> A[E];
-        auto PH = [&](int slot, int row) -> T & { return ph[slot * L + row]; };
+#define PH(slot, row) ph[(slot) * L + (row)]
         // (u, v)
-        k3_load_pair<T, L, E>(A, F[0], false, F[1], false, g.Kz, sz, q, ok);
+        k3_load_pair<T, L, E>(A, F(0), false, F(1), false, g.Kz, sz, q, ok);
         fft<T, L, E, true>(A, sm, q, tw);
 #pragma unroll
         for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); PH(0, row) = A[e].x; PH(1, row) = A[e].y; }
         // (w, du/dz)
-        k3_load_pair<T, L, E>(A, F[2], false, F[0], true, g.Kz, sz, q, ok);
+        k3_load_pair<T, L, E>(A, F(2), false, F(0), true, g.Kz, sz, q, ok);
         fft<T, L, E, true>(A, sm, q, tw);
 #pragma unroll
         for (int e = 0; e < E; e++) {
@@ -386,64 +389,64 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
             const T ww = A[e].x;
             PH(2, row) = ww;
             cfl_update<T>(mx, PH(0, row), PH(1, row), ww, c);
-            cxv[e] = ww * A[e].y;
-            if (MODE == MODE_LES) PH(6, row) = A[e].y; // a13 = du/dz (+ dw/dx below)
+            PH(3, row) = ww * A[e].y;
+            if (MODE == MODE_LES) PH(9, row) = A[e].y; // a13 = du/dz (+ dw/dx below)
         }
         // (du/dx, du/dy)
-        k3_load_pair<T, L, E>(A, F[3], false, F[6], false, g.Kz, sz, q, ok);
+        k3_load_pair<T, L, E>(A, F(3), false, F(6), false, g.Kz, sz, q, ok);
         fft<T, L, E, true>(A, sm, q, tw);
 #pragma unroll
         for (int e = 0; e < E; e++) {
             const int row = out_row<L, E, true>(q, e);
-            cxv[e] = PH(0, row) * A[e].x + PH(1, row) * A[e].y + cxv[e];
-            if (MODE == MODE_LES) { PH(3, row) = A[e].x; PH(4, row) = A[e].y; } // a11, a12 (partial)
+            PH(3, row) = PH(0, row) * A[e].x + PH(1, row) * A[e].y + PH(3, row);
+            if (MODE == MODE_LES) { PH(6, row) = A[e].x; PH(7, row) = A[e].y; } // a11, a12 (partial)
         }
         // (dv/dx, dv/dy)
-        k3_load_pair<T, L, E>(A, F[4], false, F[7], false, g.Kz, sz, q, ok);
+        k3_load_pair<T, L, E>(A, F(4), false, F(7), false, g.Kz, sz, q, ok);
         fft<T, L, E, true>(A, sm, q, tw);
 #pragma unroll
         for (int e = 0; e < E; e++) {
             const int row = out_row<L, E, true>(q, e);
-            cyv[e] = PH(0, row) * A[e].x + PH(1, row) * A[e].y;
-            if (MODE == MODE_LES) { PH(4, row) = PH(4, row) + A[e].x; PH(5, row) = A[e].y; } // a12, a22
+            PH(4, row) = PH(0, row) * A[e].x + PH(1, row) * A[e].y;
+            if (MODE == MODE_LES) { PH(7, row) = PH(7, row) + A[e].x; PH(8, row) = A[e].y; } // a12, a22
         }
         // (dw/dx, dw/dy)
-        k3_load_pair<T, L, E>(A, F[5], false, F[8], false, g.Kz, sz, q, ok);
+        k3_load_pair<T, L, E>(A, F(5), false, F(8), false, g.Kz, sz, q, ok);
         fft<T, L, E, true>(A, sm, q, tw);
 #pragma unroll
         for (int e = 0; e < E; e++) {
             const int row = out_row<L, E, true>(q, e);
-            czv[e] = PH(0, row) * A[e].x + PH(1, row) * A[e].y;
-            if (MODE == MODE_LES) { PH(6, row) = PH(6, row) + A[e].x; PH(7, row) = A[e].y; } // a13, a23 (partial)
+            PH(5, row) = PH(0, row) * A[e].x + PH(1, row) * A[e].y;
+            if (MODE == MODE_LES) { PH(9, row) = PH(9, row) + A[e].x; PH(10, row) = A[e].y; } // a13, a23 (partial)
         }
         // (dv/dz, dw/dz)
-        k3_load_pair<T, L, E>(A, F[1], true, F[2], true, g.Kz, sz, q, ok);
+        k3_load_pair<T, L, E>(A, F(1), true, F(2), true, g.Kz, sz, q, ok);
         fft<T, L, E, true>(A, sm, q, tw);
 #pragma unroll
         for (int e = 0; e < E; e++) {
             const int row = out_row<L, E, true>(q, e);
             const T ww = PH(2, row);
-            cyv[e] = cyv[e] + ww * A[e].x;
-            czv[e] = czv[e] + ww * A[e].y;
-            if (MODE == MODE_LES) { PH(7, row) = PH(7, row) + A[e].x; PH(8, row) = A[e].y; } // a23, a33
+            PH(4, row) = PH(4, row) + ww * A[e].x;
+            PH(5, row) = PH(5, row) + ww * A[e].y;
+            if (MODE == MODE_LES) { PH(10, row) = PH(10, row) + A[e].x; PH(11, row) = A[e].y; } // a23, a33
         }
         if (!ok) { mx[0] = mx[1] = mx[2] = mx[3] = 0.0; }
         block_max4<T>(mx, ds);
         if constexpr (MODE == MODE_ADV) {
 #pragma unroll
-            for (int e = 0; e < E; e++) A[e] = mk<T>(cxv[e], cyv[e]);
-            k3_store_pair<T, L, E>(A, sm, q, g.Kz, F[0], F[1], false, sz, ok, tw);
+            for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(PH(3, row), PH(4, row)); }
+            k3_store_pair<T, L, E>(A, sm, q, g.Kz, F(0), F(1), false, sz, ok, tw);
 #pragma unroll
-            for (int e = 0; e < E; e++) A[e] = mk<T>(czv[e], T(0));
-            k3_store_single<T, L, E>(A, sm, q, g.Kz, F[2], ok, tw);
+            for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(PH(5, row), T(0)); }
+            k3_store_single<T, L, E>(A, sm, q, g.Kz, F(2), ok, tw);
         } else {
-            // eddy viscosity and SGS stress (src/HIT_LES.cpp:130-154), kept in the a_ij slots:
-            // slot 3 t11, 4 t12, 5 t22, 6 t13, 7 t23, 8 t33
+            // eddy viscosity and SGS stress (src/HIT_LES.cpp:130-154), written over the a_ij slots:
+            // slot 6 t11, 7 t12, 8 t22, 9 t13, 10 t23, 11 t33
             const T ct = T(c.les_ct);
 #pragma unroll
             for (int e = 0; e < E; e++) {
                 const int row = out_row<L, E, true>(q, e);
-                const T a11 = PH(3, row), a12 = PH(4, row), a22 = PH(5, row), a13 = PH(6, row), a23 = PH(7, row), a33 = PH(8, row);
+                const T a11 = PH(6, row), a12 = PH(7, row), a22 = PH(8, row), a13 = PH(9, row), a23 = PH(10, row), a33 = PH(11, row);
                 T ne = T(2.0) * a11 * a11;
                 ne += T(2.0) * a22 * a22;
                 ne += T(2.0) * a33 * a33;
@@ -451,31 +454,33 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
                 ne += a13 * a13;
                 ne += a23 * a23;
                 ne = ct * sqrt(ne);
-                PH(3, row) = T(-2.0) * ne * a11;
-                PH(4, row) = T(-1.0) * ne * a12;
-                PH(5, row) = T(-2.0) * ne * a22;
-                PH(6, row) = T(-1.0) * ne * a13;
-                PH(7, row) = T(-1.0) * ne * a23;
-                PH(8, row) = T(-2.0) * ne * a33;
+                PH(6, row) = T(-2.0) * ne * a11;
+                PH(7, row) = T(-1.0) * ne * a12;
+                PH(8, row) = T(-2.0) * ne * a22;
+                PH(9, row) = T(-1.0) * ne * a13;
+                PH(10, row) = T(-1.0) * ne * a23;
+                PH(11, row) = T(-2.0) * ne * a33;
             }
             // outputs: 0 G_x = conv_x + i kz t13, 1 G_y, 2 G_z, 3 t11, 4 t12, 5 t13, 6 t22, 7 t23
 #pragma unroll
-            for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(cxv[e], PH(6, row)); }
-            k3_store_pair<T, L, E>(A, sm, q, g.Kz, F[0], F[5], true, sz, ok, tw);
+            for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(PH(3, row), PH(9, row)); }
+            k3_store_pair<T, L, E>(A, sm, q, g.Kz, F(0), F(5), true, sz, ok, tw);
 #pragma unroll
-            for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(cyv[e], PH(7, row)); }
-            k3_store_pair<T, L, E>(A, sm, q, g.Kz, F[1], F[7], true, sz, ok, tw);
+            for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(PH(4, row), PH(10, row)); }
+            k3_store_pair<T, L, E>(A, sm, q, g.Kz, F(1), F(7), true, sz, ok, tw);
 #pragma unroll
-            for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(czv[e], PH(8, row)); }
-            k3_store_pair<T, L, E>(A, sm, q, g.Kz, F[2], nullptr, true, sz, ok, tw);
+            for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(PH(5, row), PH(11, row)); }
+            k3_store_pair<T, L, E>(A, sm, q, g.Kz, F(2), nullptr, true, sz, ok, tw);
 #pragma unroll
-            for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(PH(3, row), PH(4, row)); }
-            k3_store_pair<T, L, E>(A, sm, q, g.Kz, F[3], F[4], false, sz, ok, tw);
+            for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(PH(6, row), PH(7, row)); }
+            k3_store_pair<T, L, E>(A, sm, q, g.Kz, F(3), F(4), false, sz, ok, tw);
 #pragma unroll
-            for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(PH(5, row), T(0)); }
-            k3_store_single<T, L, E>(A, sm, q, g.Kz, F[6], ok, tw);
+            for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(PH(8, row), T(0)); }
+            k3_store_single<T, L, E>(A, sm, q, g.Kz, F(6), ok, tw);
         }
+#undef PH
     }
+#undef F
 }
 
 // ===========================================================================
@@ -483,7 +488,7 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
 // LES: G_i += i ky t_i2 (SGS divergence, y part).
 // ===========================================================================
 template <typename T, int L, int E, int P, int MODE>
-__global__ void __launch_bounds__(P *(L / E)) k4_fwd_y(Geo g, const cx<T> *__restrict__ in, cx<T> *__restrict__ out,
+__global__ void __launch_bounds__(P *(L / E), 2) k4_fwd_y(Geo g, const cx<T> *__restrict__ in, cx<T> *__restrict__ out,
                                                        const cx<T> *__restrict__ tw) {
     extern __shared__ __align__(16) unsigned char smraw[];
     const int tid = threadIdx.x, p = tid % P, q = tid / P;
@@ -539,108 +544,131 @@ __global__ void __launch_bounds__(P *(L / E)) k4_fwd_y(Geo g, const cx<T> *__res
 }
 
 // ===========================================================================
-// K5: forward transform along x + the spectral sweep of the step
-// (src/HIT_LES.cpp:196-242 R vector, 243-278 constant-power forcing,
-//  295-339 predictor, 346-359 projection).  Block = (kz chunk, iy).
-// LES: G_i += i kx t_i1 (SGS divergence, x part).
+// K5: forward transform along x with kx truncation into the compact layout
+// (S0).  Block = (kz chunk, iy).  LES: G_i += i kx t_i1 (SGS divergence, x part).
 // ===========================================================================
-template <typename T, int L, int E, int P, int MODE, bool SELF>
-__global__ void __launch_bounds__(P *(L / E)) k5_fwd_x_sweep(Geo g, const cx<T> *__restrict__ in, cx<T> *__restrict__ U,
-                                                             cx<T> *__restrict__ R, cx<T> *__restrict__ Uprev,
-                                                             StepConsts c, const DevScalars *__restrict__ ds,
-                                                             const cx<T> *__restrict__ tw) {
+template <typename T, int L, int E, int P, int MODE>
+__global__ void __launch_bounds__(P *(L / E), 2) k5_fwd_x(Geo g, const cx<T> *__restrict__ in, cx<T> *__restrict__ G,
+                                                          const cx<T> *__restrict__ tw) {
     extern __shared__ __align__(16) unsigned char smraw[];
     const int tid = threadIdx.x, p = tid % P, q = tid / P;
     const int iy = blockIdx.y, kz = blockIdx.x * P + p;
     const bool ok = kz < g.Kz;
     SmRowMajor<T, P> sm{reinterpret_cast<cx<T> *>(smraw), p};
-    cx<T> G[3][E];
     const long long col = (long long)iy * g.Mx * g.Kz + kz;
-#pragma unroll
-    for (int f = 0; f < 3; f++) {
+    auto load_fft = [&](cx<T>(&r)[E], int f) {
         const cx<T> *src = in + (long long)f * g.S1 + col;
 #pragma unroll
-        for (int e = 0; e < E; e++) G[f][e] = ok ? src[(long long)in_row<L, E, false>(q, e) * g.Kz] : zero<T>();
-        fft<T, L, E, false>(G[f], sm, q, tw);
+        for (int e = 0; e < E; e++) r[e] = ok ? src[(long long)in_row<L, E, false>(q, e) * g.Kz] : zero<T>();
+        fft<T, L, E, false>(r, sm, q, tw);
+    };
+#pragma unroll 1
+    for (int f = 0; f < 3; f++) {
+        cx<T> r[E];
+        load_fft(r, f);
         if constexpr (MODE == MODE_LES) {
             cx<T> t[E];
-            const cx<T> *ts = in + (long long)(3 + f) * g.S1 + col;
-#pragma unroll
-            for (int e = 0; e < E; e++) t[e] = ok ? ts[(long long)in_row<L, E, false>(q, e) * g.Kz] : zero<T>();
-            fft<T, L, E, false>(t, sm, q, tw);
+            load_fft(t, 3 + f); // t11, t21=t12, t31=t13
 #pragma unroll
             for (int e = 0; e < E; e++) {
                 const int m1 = ffreq(out_row<L, E, false>(q, e), L);
-                G[f][e] = G[f][e] + mul_i(T(g.sx * m1) * t[e]);
+                r[e] = r[e] + mul_i(T(g.sx * m1) * t[e]);
+            }
+        }
+        if (ok) {
+            cx<T> *o = G + (long long)f * g.S0 + (long long)iy * g.Kx * g.Kz + kz;
+#pragma unroll
+            for (int e = 0; e < E; e++) {
+                const int m1 = ffreq(out_row<L, E, false>(q, e), L);
+                if (m1 <= g.hx && m1 >= -g.hx) o[(long long)(m1 >= 0 ? m1 : m1 + g.Kx) * g.Kz] = r[e];
             }
         }
     }
-    if (!ok) return;
+}
+
+// ===========================================================================
+// K6: the spectral sweep of the step over the compact state (streaming; every
+// load of a mode is issued before any store):
+//   src/HIT_LES.cpp:196-242  R = -conv (0 at k=0) - nu k^2 u [- div tau] [+ Coriolis]
+//   src/HIT_LES.cpp:243-278  constant-power forcing (when enabled)
+//   src/HIT_LES.cpp:295-339  predictor: AB2, or the kappa scheme
+//   src/HIT_LES.cpp:346-359  projection  u -= k (k.u)/k^2
+// G holds the un-normalised nonlinear term (x1/M^3 here).  Kappa scheme: the
+// new state is written over the u^{n-1} buffer Un1 and the caller swaps U/Un1.
+// ===========================================================================
+template <typename T, bool SELF>
+__global__ void __launch_bounds__(256) k6_sweep(Geo g, const cx<T> *__restrict__ G, const cx<T> *U, cx<T> *R, cx<T> *Uout,
+                                                const cx<T> *Un1, StepConsts c, const DevScalars *__restrict__ ds) {
+    const int iy = blockIdx.y;
+    const int n = g.Kx * g.Kz;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int ix = t / g.Kz, kz = t - ix * g.Kz;
+    const long long idx = (long long)iy * n + t;
+    const long long S0 = g.S0;
+    // loads first
+    cx<T> gg[3], uu[3], r0[3], up[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) { gg[i] = G[i * S0 + idx]; uu[i] = U[i * S0 + idx]; r0[i] = R[i * S0 + idx]; }
     const double nu = ds->nu, dt = ds->dt, kap = ds->kappa, alpha = ds->alpha;
     const bool first = ds->iter == 0;
-    const int m2 = iy <= g.hy ? iy : iy - g.Ky;
-    const long long k2 = (long long)g.sy * m2, k3 = (long long)g.sz * kz;
-    const long long S0 = g.S0;
+    if (SELF) {
 #pragma unroll
-    for (int e = 0; e < E; e++) {
-        const int m1 = ffreq(out_row<L, E, false>(q, e), L);
-        if (m1 > g.hx || m1 < -g.hx) continue;
-        const long long idx = ((long long)iy * g.Kx + (m1 >= 0 ? m1 : m1 + g.Kx)) * g.Kz + kz;
-        const long long k1 = (long long)g.sx * m1;
-        const double rad2 = (double)(k1 * k1 + k2 * k2 + k3 * k3);
-        const bool mean = !(rad2 > 0.0);
-        const double ct = nu * rad2;
-        double ur[3], ui[3], rr[3], ri[3];
+        for (int i = 0; i < 3; i++) up[i] = first ? uu[i] : Un1[i * S0 + idx];
+    }
+    const int m1 = ix <= g.hx ? ix : ix - g.Kx, m2 = iy <= g.hy ? iy : iy - g.Ky;
+    const long long k1 = (long long)g.sx * m1, k2 = (long long)g.sy * m2, k3 = (long long)g.sz * kz;
+    const double rad2 = (double)(k1 * k1 + k2 * k2 + k3 * k3);
+    const bool mean = !(rad2 > 0.0);
+    const double ct = nu * rad2;
+    double ur[3], ui[3], rr[3], ri[3];
 #pragma unroll
-        for (int i = 0; i < 3; i++) {
-            const cx<T> uu = U[i * S0 + idx];
-            ur[i] = uu.x; ui[i] = uu.y;
-            const double gr = mean ? 0.0 : (double)G[i][e].x * c.inv_norm;
-            const double gi = mean ? 0.0 : (double)G[i][e].y * c.inv_norm;
-            rr[i] = -gr - ct * ur[i];
-            ri[i] = -gi - ct * ui[i];
+    for (int i = 0; i < 3; i++) {
+        ur[i] = uu[i].x; ui[i] = uu[i].y;
+        const double gr = mean ? 0.0 : (double)gg[i].x * c.inv_norm;
+        const double gi = mean ? 0.0 : (double)gg[i].y * c.inv_norm;
+        rr[i] = -gr - ct * ur[i];
+        ri[i] = -gi - ct * ui[i];
+    }
+    if (c.rotating) {
+        rr[0] += 2 * (c.omega_z * ur[1] - c.omega_y * ur[2]); ri[0] += 2 * (c.omega_z * ui[1] - c.omega_y * ui[2]);
+        rr[1] += 2 * (c.omega_x * ur[2] - c.omega_z * ur[0]); ri[1] += 2 * (c.omega_x * ui[2] - c.omega_z * ui[0]);
+        rr[2] += 2 * (c.omega_y * ur[0] - c.omega_x * ur[1]); ri[2] += 2 * (c.omega_y * ui[0] - c.omega_x * ui[1]);
+    }
+    if (c.eps_on) {
+        const int K = (int)round(sqrt(rad2));
+        if (c.eps_kmin <= K && K <= c.eps_kmax) {
+#pragma unroll
+            for (int i = 0; i < 3; i++) { rr[i] += alpha * ur[i]; ri[i] += alpha * ui[i]; }
+        } else if (K == 0) {
+#pragma unroll
+            for (int i = 0; i < 3; i++) { rr[i] = 0.0; ri[i] = 0.0; }
         }
-        if (c.rotating) {
-            rr[0] += 2 * (c.omega_z * ur[1] - c.omega_y * ur[2]); ri[0] += 2 * (c.omega_z * ui[1] - c.omega_y * ui[2]);
-            rr[1] += 2 * (c.omega_x * ur[2] - c.omega_z * ur[0]); ri[1] += 2 * (c.omega_x * ui[2] - c.omega_z * ui[0]);
-            rr[2] += 2 * (c.omega_y * ur[0] - c.omega_x * ur[1]); ri[2] += 2 * (c.omega_y * ui[0] - c.omega_x * ui[1]);
+    }
+    double sr[3], si[3];
+    const double k05 = SELF ? 1.0 / (kap + 0.5) : 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        if (SELF) {
+            sr[i] = k05 * (2.0 * kap * ur[i] + dt * ((1.0 + kap) * rr[i] - kap * (double)r0[i].x) - (kap - 0.5) * (double)up[i].x);
+            si[i] = k05 * (2.0 * kap * ui[i] + dt * ((1.0 + kap) * ri[i] - kap * (double)r0[i].y) - (kap - 0.5) * (double)up[i].y);
+        } else {
+            sr[i] = ur[i] + dt * (1.5 * rr[i] - 0.5 * (double)r0[i].x);
+            si[i] = ui[i] + dt * (1.5 * ri[i] - 0.5 * (double)r0[i].y);
         }
-        if (c.eps_on) {
-            const int K = (int)round(sqrt(rad2));
-            if (c.eps_kmin <= K && K <= c.eps_kmax) {
+    }
+    if (rad2 > 0.0) {
+        const double kk[3] = {(double)k1, (double)k2, (double)k3};
+        const double inv = 1.0 / rad2;
+        const double ar = (kk[0] * sr[0] + kk[1] * sr[1] + kk[2] * sr[2]) * inv;
+        const double ai = (kk[0] * si[0] + kk[1] * si[1] + kk[2] * si[2]) * inv;
 #pragma unroll
-                for (int i = 0; i < 3; i++) { rr[i] += alpha * ur[i]; ri[i] += alpha * ui[i]; }
-            } else if (K == 0) {
+        for (int i = 0; i < 3; i++) { sr[i] -= ar * kk[i]; si[i] -= ai * kk[i]; }
+    }
 #pragma unroll
-                for (int i = 0; i < 3; i++) { rr[i] = 0.0; ri[i] = 0.0; }
-            }
-        }
-        double sr[3], si[3];
-#pragma unroll
-        for (int i = 0; i < 3; i++) {
-            const cx<T> r0 = R[i * S0 + idx];
-            if (SELF) {
-                double pr = ur[i], pi = ui[i];
-                if (!first) { const cx<T> up = Uprev[i * S0 + idx]; pr = up.x; pi = up.y; }
-                const double k05 = 1.0 / (kap + 0.5);
-                sr[i] = k05 * (2.0 * kap * ur[i] + dt * ((1.0 + kap) * rr[i] - kap * (double)r0.x) - (kap - 0.5) * pr);
-                si[i] = k05 * (2.0 * kap * ui[i] + dt * ((1.0 + kap) * ri[i] - kap * (double)r0.y) - (kap - 0.5) * pi);
-                Uprev[i * S0 + idx] = mk<T>(T(ur[i]), T(ui[i]));
-            } else {
-                sr[i] = ur[i] + dt * (1.5 * rr[i] - 0.5 * (double)r0.x);
-                si[i] = ui[i] + dt * (1.5 * ri[i] - 0.5 * (double)r0.y);
-            }
-            R[i * S0 + idx] = mk<T>(T(rr[i]), T(ri[i]));
-        }
-        if (rad2 > 0.0) {
-            const double kk[3] = {(double)k1, (double)k2, (double)k3};
-            const double ar = (kk[0] * sr[0] + kk[1] * sr[1] + kk[2] * sr[2]) / rad2;
-            const double ai = (kk[0] * si[0] + kk[1] * si[1] + kk[2] * si[2]) / rad2;
-#pragma unroll
-            for (int i = 0; i < 3; i++) { sr[i] -= ar * kk[i]; si[i] -= ai * kk[i]; }
-        }
-#pragma unroll
-        for (int i = 0; i < 3; i++) U[i * S0 + idx] = mk<T>(T(sr[i]), T(si[i]));
+    for (int i = 0; i < 3; i++) {
+        R[i * S0 + idx] = mk<T>(T(rr[i]), T(ri[i]));
+        Uout[i * S0 + idx] = mk<T>(T(sr[i]), T(si[i]));
     }
 }
 

@@ -170,14 +170,28 @@ template <int L, int MODE> static cudaError_t launch_k4(spns_handle *h) {
     kern<<<grid, S::THREADS, S::SMEM_ROW, h->st>>>(h->g, (const cx<T64> *)h->B2, (cx<T64> *)h->B1, (const cx<T64> *)h->tw[L]);
     return cudaGetLastError();
 }
-template <int L, int MODE, bool SELF> static cudaError_t launch_k5(spns_handle *h) {
+template <int L, int MODE> static cudaError_t launch_k5(spns_handle *h) {
     using S = Shape<T64, L>;
-    auto kern = k5_fwd_x_sweep<T64, L, S::E, S::P, MODE, SELF>;
+    auto kern = k5_fwd_x<T64, L, S::E, S::P, MODE>;
     cudaError_t e = set_smem(kern, S::SMEM_ROW);
     if (e != cudaSuccess) return e;
     dim3 grid((h->g.Kz + S::P - 1) / S::P, h->g.Ky);
-    kern<<<grid, S::THREADS, S::SMEM_ROW, h->st>>>(h->g, (const cx<T64> *)h->B1, (cx<T64> *)h->U, (cx<T64> *)h->R,
-                                                  (cx<T64> *)h->Up, h->c, h->ds, (const cx<T64> *)h->tw[L]);
+    kern<<<grid, S::THREADS, S::SMEM_ROW, h->st>>>(h->g, (const cx<T64> *)h->B1, (cx<T64> *)h->B2, (const cx<T64> *)h->tw[L]);
+    return cudaGetLastError();
+}
+// Spectral sweep; with the kappa scheme the new state goes into the u^{n-1}
+// buffer and the two state buffers are swapped after the launch.
+static cudaError_t launch_k6(spns_handle *h) {
+    const int n = h->g.Kx * h->g.Kz;
+    dim3 grid((n + 255) / 256, h->g.Ky);
+    if (h->a.isSelfAdaptive) {
+        k6_sweep<T64, true><<<grid, 256, 0, h->st>>>(h->g, (const cx<T64> *)h->B2, (const cx<T64> *)h->U, (cx<T64> *)h->R,
+                                                     (cx<T64> *)h->Up, (const cx<T64> *)h->Up, h->c, h->ds);
+        std::swap(h->U, h->Up);
+    } else {
+        k6_sweep<T64, false><<<grid, 256, 0, h->st>>>(h->g, (const cx<T64> *)h->B2, (const cx<T64> *)h->U, (cx<T64> *)h->R,
+                                                      (cx<T64> *)h->U, nullptr, h->c, h->ds);
+    }
     return cudaGetLastError();
 }
 
@@ -261,9 +275,10 @@ static int step_once(spns_handle *h) {
     DISPATCH(h->g.Mz, LAUNCH((launch_k3<LL, MD>(h, nullptr))));                               \
     MARK("k4_fwd_y");                                                                         \
     DISPATCH(h->g.My, LAUNCH((launch_k4<LL, MD>(h))));                                        \
-    MARK("k5_fwd_x_sweep");                                                                   \
-    if (h->a.isSelfAdaptive) { DISPATCH(h->g.Mx, LAUNCH((launch_k5<LL, MD, true>(h)))); }     \
-    else { DISPATCH(h->g.Mx, LAUNCH((launch_k5<LL, MD, false>(h)))); }
+    MARK("k5_fwd_x");                                                                         \
+    DISPATCH(h->g.Mx, LAUNCH((launch_k5<LL, MD>(h))));                                        \
+    MARK("k6_sweep");                                                                         \
+    LAUNCH(launch_k6(h));
     if (mode == MODE_LES) { STEP_PASSES(MODE_LES) }
     else if (mode == MODE_ROT) { STEP_PASSES(MODE_ROT) }
     else { STEP_PASSES(MODE_ADV) }
@@ -273,7 +288,7 @@ static int step_once(spns_handle *h) {
     CKL();
     MARK(nullptr);
     if (prof) { if (h->prof_steps == 0) h->prof_nk = slot - 1; h->prof_steps++; }
-    h->kernels_per_step = nk + 7;
+    h->kernels_per_step = nk + 8;
     return SPNS_OK;
 #undef MARK
 }
