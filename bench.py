@@ -153,12 +153,8 @@ def dist_setup(n_gpus: int):
 
 
 def reduce_max(dist, value: float) -> float:
-    if dist is None:
-        return value
-    import torch
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from spns_b200.replicas import max_over_ranks
+    return max_over_ranks(value, dist, "cuda")
 
 
 def barrier(dist):
@@ -290,8 +286,9 @@ def run_gpu(args):
         if dist is not None:
             dist.destroy_process_group()
         return 0
-    value = world * args.steps / (ms_max / 1e3)
-    e2e_value = world * args.steps / e2e_max
+    from spns_b200.replicas import whole_job_rate
+    value = whole_job_rate(world, args.steps, ms_max / 1e3)
+    e2e_value = whole_job_rate(world, args.steps, e2e_max)
     # roofline of the dominant kernel
     bytes_per, sizes = algorithmic_bytes(N)
     mean_ms = per.mean(axis=0)
