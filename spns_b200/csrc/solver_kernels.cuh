@@ -727,16 +727,16 @@ __device__ __forceinline__ void recalc_dt(const StepConsts &c, DevScalars *ds) {
     }
 }
 
-__global__ void k_recalc_dt(StepConsts c, DevScalars *ds) { recalc_dt(c, ds); }
+static __global__ void k_recalc_dt(StepConsts c, DevScalars *ds) { recalc_dt(c, ds); }
 
 // End of New_Fractional_Step_Method (src/HIT_LES.cpp:19-24).
-__global__ void k_finish_step(StepConsts c, DevScalars *ds) {
+static __global__ void k_finish_step(StepConsts c, DevScalars *ds) {
     recalc_dt(c, ds);
     ds->time = ds->time + ds->dt;
     ds->iter += 1;
 }
 
-__global__ void k_reset_max(DevScalars *ds) {
+static __global__ void k_reset_max(DevScalars *ds) {
     for (int i = 0; i < 4; i++) ds->max_bits[i] = 0ull;
     ds->sumsq_phys = 0.0;
 }
@@ -778,7 +778,7 @@ __global__ void k_shell_sums(Geo g, const cx<T> *__restrict__ u, const cx<T> *__
 
 // Totals of the shell sums: Ek_Tot over K=0..Kmax, Ok_Tot over K=1..Kmax.
 // what: 0 energy only, 1 energy+enstrophy (+ReLambda), 2 Forcing_Reynolds_Lambda.
-__global__ void k_totals(const double *Ek, const double *Om, int Kmax, DevScalars *ds, int what, double relambda) {
+static __global__ void k_totals(const double *Ek, const double *Om, int Kmax, DevScalars *ds, int what, double relambda) {
     double e = 0.0, o = 0.0;
     for (int K = 0; K <= Kmax; K++) e += Ek[K];
     for (int K = 1; K <= Kmax; K++) o += Om[K];
@@ -790,14 +790,14 @@ __global__ void k_totals(const double *Ek, const double *Om, int Kmax, DevScalar
 
 // Constant-power forcing coefficient alpha = eps/(2 E_f), E_f the energy of
 // shells [kmin,kmax] of the current state (src/HIT_LES.cpp:250-256).
-__global__ void k_eps_alpha(const double *Ek, int kmin, int kmax, double eps, DevScalars *ds) {
+static __global__ void k_eps_alpha(const double *Ek, int kmin, int kmax, double eps, DevScalars *ds) {
     double Ef = 0.0;
     for (int K = kmin; K <= kmax; K++) Ef += Ek[K];
     ds->alpha = Ef > 1e-30 ? eps / (2.0 * Ef) : 0.0;
 }
 
 // src/HIT_LES.cpp:417-419: FT[K] = sqrt(Forced_Ek[K]/Ek[K]).
-__global__ void k_forcing_factors(const double *Ek, const double *Forced, int last_eff, double *FT) {
+static __global__ void k_forcing_factors(const double *Ek, const double *Forced, int last_eff, double *FT) {
     for (int K = threadIdx.x; K <= last_eff; K += blockDim.x) FT[K] = Ek[K] > 0.0 ? sqrt(Forced[K] / Ek[K]) : 0.0;
 }
 
@@ -841,7 +841,7 @@ __global__ void k_conj_correction(Geo g, cx<T> *u, cx<T> *v, cx<T> *w) {
 // Direct DFT along one axis (initial-field transform of the input file; init only).
 // in: complex lines, out: complex lines; out[o][k] = sum_n in[o][n] * w^(k*n mod N).
 // Line l of `nl` lines starts at (l / inner)*outer_stride + (l % inner), element stride `es`.
-__global__ void k_dft_axis(const double2 *__restrict__ in, double2 *__restrict__ out, int N, int nk, const int *__restrict__ kidx,
+static __global__ void k_dft_axis(const double2 *__restrict__ in, double2 *__restrict__ out, int N, int nk, const int *__restrict__ kidx,
                            long long nl, long long inner, long long in_outer, long long out_outer, long long es_in,
                            long long es_out, const double2 *__restrict__ twN) {
     const long long tot = nl * nk;

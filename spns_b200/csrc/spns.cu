@@ -80,6 +80,9 @@ struct spns_handle {
 
 static thread_local std::string g_create_error;
 
+// Error text for calls that have no handle (reported by spns_last_error(NULL)).
+__attribute__((visibility("hidden"))) void spns_set_handleless_error(const char *msg) { g_create_error = msg; }
+
 static int fail(spns_handle *h, int code, const char *fmt, ...) {
     char buf[1024];
     va_list ap;

@@ -30,6 +30,7 @@ EXPORTED_SYMBOLS = (
     "spns_spectral_dims", "spns_physical_dims", "spns_get_spectral", "spns_set_spectral", "spns_get_physical",
     "spns_device_state", "spns_stream", "spns_kernels_per_step", "spns_last_error", "spns_status_string",
     "spns_fft1d_batch_f64", "spns_profile_begin", "spns_profile_read", "spns_profile_kernel_name",
+    "spns_energy_cascade_noalloc_f64",
 )
 
 
@@ -111,6 +112,7 @@ def lib():
         L.spns_profile_read.argtypes = [vp, C.POINTER(C.c_float), i, ip, ip]
         L.spns_profile_kernel_name.argtypes = [vp, i]
         L.spns_profile_kernel_name.restype = C.c_char_p
+        L.spns_energy_cascade_noalloc_f64.argtypes = [vp, i, i, i, i, i, i, dp, i, dp, vp]
         _lib = L
     return _lib
 
