@@ -53,13 +53,15 @@ def box_args(N: int, self_adaptive: bool = True):
                    isRotating=False, isLES=False, isComplexConjugateCorrected=False, isSelfAdaptive=self_adaptive)
 
 
-def algorithmic_bytes(N: int, self_adaptive: bool = True, word: int = 16, form: str = "advective"):
+def algorithmic_bytes(N: int, self_adaptive: bool = True, word: int = 16, form: str = "rotational"):
     """Bytes each kernel must move once (arrays read + written, each counted once).
 
     S0 = compact spectral field, S1 = after the x transform, S2 = after the y
-    transform (complex elements of `word` bytes).  Advective form: K1 3 S0 -> 6 S1,
-    K2 6 S1 -> 9 S2, K3 9 S2 -> 3 S2, K4 3 S2 -> 3 S1, K5 3 S1 -> 3 S0 (nonlinear
-    term G), K6 reads G, u, R^{n-1} (+ u^{n-1}) and writes R^n, u^{n+1}."""
+    transform (complex elements of `word` bytes).  Rotational form (default, exact
+    with the edge correction): K1 3 S0 -> 5 S1, K2 5 S1 -> 6 S2, K3 6 S2 -> 3 S2;
+    advective form: 3 S0 -> 6 S1, 6 S1 -> 9 S2, 9 S2 -> 3 S2.  Then K4 3 S2 -> 3 S1,
+    K5 3 S1 -> 3 S0 (nonlinear term G), K6 reads G, u, R^{n-1} (+ u^{n-1}) and writes
+    R^n, u^{n+1}.  The edge correction moves O(M^2) bytes (negligible)."""
     h = N // 2
     K, M, Kz = 2 * h + 1, (3 * N) // 2, h + 1
     S0, S1, S2 = K * K * Kz, K * M * Kz, M * M * Kz
@@ -312,7 +314,7 @@ def run_gpu(args):
                    "N": N, "fft_grid": (3 * N) // 2, "parallelism": f"replicas x{world}",
                    "l2": f"inputs larger than L2 (state {3 * sizes['S0'] * 16 / 1e9:.1f} GB, work buffers "
                          f"{(6 * sizes['S1'] + 9 * sizes['S2']) * 16 / 1e9:.1f} GB)",
-                   "nonlinear_form": "advective (u.grad u, as the reference)",
+                   "nonlinear_form": "rotational + exact +-N/2 aliasing correction (= the reference's u.grad u after projection)",
                    "finite": finite},
         "clocks": clk.summary(),
         "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": 0,

@@ -56,11 +56,13 @@ typedef struct spns_hit_args {
     double fixed_dt;         /* >0: constant time step instead of the CFL/self-adaptive one */
     double eps_forcing;      /* >0: constant-power forcing on shells [eps_kmin, eps_kmax]   */
     int eps_kmin, eps_kmax;  /*     (the disabled block src/HIT_LES.cpp:243-278, eps_in=eps) */
-    int nonlinear_form;      /* DNS only: 0 = advective u.grad(u) as the reference
-                                (src/HIT_LES.cpp:74-125, 12 inverse transforms), 1 = rotational
-                                omega x u (6 inverse transforms; equal to the advective form
-                                up to a gradient, hence identical after the projection only while
-                                the aliased +-N/2 modes of the 3/2 rule carry no energy) */
+    int nonlinear_form;      /* DNS only.  0 (default): rotational omega x u (6 inverse
+                                transforms) plus the exact aliasing correction of the +-N/2
+                                planes, which equals the reference's advective u.grad(u)
+                                (src/HIT_LES.cpp:74-125) after the projection;
+                                1: rotational without the correction (equal only while the
+                                +-N/2 modes carry no energy); 2: advective, 12 inverse
+                                transforms, the reference's arithmetic */
 } spns_hit_args;
 
 typedef struct spns_handle spns_handle;

@@ -4,6 +4,7 @@
 // (src/HIT_LES.h of adalbal/SpNS); see include/spns.h for the mapping.
 #include "spns.h"
 #include "solver_kernels.cuh"
+#include "edge_kernels.cuh"
 
 #include <cuda_runtime.h>
 
@@ -69,6 +70,8 @@ struct spns_handle {
     double *FT = nullptr, *forced = nullptr;
     int forced_cap = 0;
     double *phys = nullptr;
+    double2 *edge = nullptr;                         // edge-correction planes (rotational form)
+    bool edge_axis[3] = {false, false, false};       // axes whose +-N/2 planes alias (M = 3h)
     std::map<int, double2 *> tw;                     // twiddle tables per length
     std::string err;
     int kernels_per_step = 0;
@@ -198,6 +201,25 @@ static cudaError_t launch_k6(spns_handle *h) {
     return cudaGetLastError();
 }
 
+// Batched 1-D FFTs for the 2-D edge planes.
+template <int L, bool INV> static cudaError_t launch_lines(spns_handle *h, double2 *data, long long batch) {
+    using S = Shape<T64, L>;
+    auto kern = k_lines<T64, L, S::E, S::P, INV>;
+    cudaError_t e = set_smem(kern, S::SMEM_PEN);
+    if (e != cudaSuccess) return e;
+    kern<<<(unsigned)((batch + S::P - 1) / S::P), S::THREADS, S::SMEM_PEN, h->st>>>((cx<T64> *)data, batch, (const cx<T64> *)h->tw[L]);
+    return cudaGetLastError();
+}
+template <int L, bool INV> static cudaError_t launch_cols(spns_handle *h, double2 *data, int ncols, int nbatch) {
+    using S = Shape<T64, L>;
+    auto kern = k_cols<T64, L, S::E, S::P, INV>;
+    cudaError_t e = set_smem(kern, S::SMEM_ROW);
+    if (e != cudaSuccess) return e;
+    dim3 grid((ncols + S::P - 1) / S::P, nbatch);
+    kern<<<grid, S::THREADS, S::SMEM_ROW, h->st>>>((cx<T64> *)data, ncols, (const cx<T64> *)h->tw[L]);
+    return cudaGetLastError();
+}
+
 #define DISPATCH(Lval, call)                                                                 \
     switch (Lval) {                                                                          \
     case 48: { constexpr int LL = 48; call; } break;                                         \
@@ -243,6 +265,35 @@ static int shell_sums(spns_handle *h, int bx, int by, int bz) {
     return SPNS_OK;
 }
 
+// Exact aliasing correction of the rotational form on the +-N/2 planes
+// (edge_kernels.cuh), added to the compact nonlinear term G held in B2.
+static int edge_correction(spns_handle *h) {
+    const Geo &g = h->g;
+    for (int axis = 0; axis < 3; axis++) {
+        if (!h->edge_axis[axis]) continue;
+        EdgePlanes ep;
+        ep.axis = axis;
+        ep.nplanes = axis == 2 ? 1 : 2;
+        ep.R = axis == 0 ? g.My : g.Mx;
+        ep.C = axis == 2 ? g.My : g.Mz;
+        const long long n = (long long)ep.R * ep.C;
+        double2 *V = h->edge, *Phi = h->edge + 3 * 2 * n;
+        const long long nb = n * 3 * ep.nplanes;
+        const int blocks = (int)std::min<long long>((nb + 255) / 256, 148 * 16);
+        k_edge_build<T64><<<blocks, 256, 0, h->st>>>(g, (const cx<T64> *)h->U, ep, (cx<T64> *)V);
+        CKL();
+        DISPATCH(ep.C, LAUNCH((launch_lines<LL, true>(h, V, (long long)ep.R * 3 * ep.nplanes))));
+        DISPATCH(ep.R, LAUNCH((launch_cols<LL, true>(h, V, ep.C, 3 * ep.nplanes))));
+        k_edge_square<T64><<<blocks, 256, 0, h->st>>>((const cx<T64> *)V, n, ep.nplanes, (cx<T64> *)Phi);
+        CKL();
+        DISPATCH(ep.C, LAUNCH((launch_lines<LL, false>(h, Phi, (long long)ep.R * ep.nplanes))));
+        DISPATCH(ep.R, LAUNCH((launch_cols<LL, false>(h, Phi, ep.C, ep.nplanes))));
+        k_edge_apply<T64><<<blocks, 256, 0, h->st>>>(g, (cx<T64> *)h->B2, ep, (const cx<T64> *)Phi);
+        CKL();
+    }
+    return SPNS_OK;
+}
+
 // Records an event before the next kernel of a profiled step.
 static void prof_mark(spns_handle *h, int slot, const char *name) {
     if (h->prof_steps >= h->prof_cap_steps) return;
@@ -265,7 +316,7 @@ static int step_once(spns_handle *h) {
         CKL();
         nk += 2;
     }
-    const int mode = h->a.isLES ? MODE_LES : h->a.nonlinear_form == 1 ? MODE_ROT : MODE_ADV;
+    const int mode = h->a.isLES ? MODE_LES : h->a.nonlinear_form == 2 ? MODE_ADV : MODE_ROT;
 #define STEP_PASSES(MD)                                                                       \
     MARK("k1_inv_x");                                                                         \
     DISPATCH(h->g.Mx, LAUNCH((launch_k1<LL, MD>(h))));                                        \
@@ -280,6 +331,11 @@ static int step_once(spns_handle *h) {
     DISPATCH(h->g.My, LAUNCH((launch_k4<LL, MD>(h))));                                        \
     MARK("k5_fwd_x");                                                                         \
     DISPATCH(h->g.Mx, LAUNCH((launch_k5<LL, MD>(h))));                                        \
+    if (MD == MODE_ROT && h->edge) {                                                          \
+        MARK("edge_correction");                                                              \
+        int r_ = edge_correction(h);                                                          \
+        if (r_) return r_;                                                                    \
+    }                                                                                         \
     MARK("k6_sweep");                                                                         \
     LAUNCH(launch_k6(h));
     if (mode == MODE_LES) { STEP_PASSES(MODE_LES) }
@@ -482,7 +538,7 @@ static int read_scalars(spns_handle *h, DevScalars *s) {
 static void free_handle(spns_handle *h) {
     if (!h) return;
     cudaFree(h->ds); cudaFree(h->U); cudaFree(h->R); cudaFree(h->Up); cudaFree(h->B1); cudaFree(h->B2);
-    cudaFree(h->bins); cudaFree(h->FT); cudaFree(h->forced); cudaFree(h->phys);
+    cudaFree(h->bins); cudaFree(h->FT); cudaFree(h->forced); cudaFree(h->phys); cudaFree(h->edge);
     for (auto &kv : h->tw) cudaFree(kv.second);
     for (auto ev : h->prof_ev) cudaEventDestroy(ev);
     if (h->st) cudaStreamDestroy(h->st);
@@ -573,16 +629,23 @@ int spns_create(const spns_hit_args *args, const double *file_uvw, spns_handle *
     // device memory
     auto cleanup = [&](int code) { free_handle(h); return code; };
     if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) return cleanup(fail(nullptr, SPNS_ERR_CUDA, "stream creation failed"));
-    const bool rot = !a.isLES && a.nonlinear_form == 1;
+    const bool rot = !a.isLES && a.nonlinear_form != 2;
     h->nB1 = rot ? 5 : 6;
     h->nB2 = rot ? 6 : 9;
+    // planes k_i = +-h alias onto each other when M_i = 3 h_i (even number of retained modes)
+    h->edge_axis[0] = g.hx > 0 && g.Mx <= 3 * g.hx;
+    h->edge_axis[1] = g.hy > 0 && g.My <= 3 * g.hy;
+    h->edge_axis[2] = g.hz > 0 && g.Mz <= 3 * g.hz;
+    const bool need_edge = rot && a.nonlinear_form == 0 && (h->edge_axis[0] || h->edge_axis[1] || h->edge_axis[2]);
     size_t s0 = sizeof(double2) * 3 * g.S0;
     bool okm = cudaMalloc(&h->ds, sizeof(DevScalars)) == cudaSuccess && cudaMalloc(&h->U, s0) == cudaSuccess &&
                cudaMalloc(&h->R, s0) == cudaSuccess &&
                (!a.isSelfAdaptive || cudaMalloc(&h->Up, s0) == cudaSuccess) &&
                cudaMalloc(&h->B1, sizeof(double2) * h->nB1 * g.S1) == cudaSuccess &&
                cudaMalloc(&h->B2, sizeof(double2) * h->nB2 * g.S2) == cudaSuccess &&
-               cudaMalloc(&h->bins, sizeof(double) * 2 * (h->last_rad_max + 1)) == cudaSuccess;
+               cudaMalloc(&h->bins, sizeof(double) * 2 * (h->last_rad_max + 1)) == cudaSuccess &&
+               (!need_edge || cudaMalloc(&h->edge, sizeof(double2) * 8 *
+                                         (size_t)std::max((long long)g.My * g.Mz, std::max((long long)g.Mx * g.Mz, (long long)g.Mx * g.My))) == cudaSuccess);
     if (!okm) { cudaGetLastError(); return cleanup(fail(nullptr, SPNS_ERR_OUT_OF_MEMORY, "device allocation failed")); }
     for (int L : {g.Mx, g.My, g.Mz})
         if (!h->tw.count(L)) {

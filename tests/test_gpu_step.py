@@ -13,10 +13,10 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-12
 
 
-def _pair(args, k41_ranks=4, **opt):
+def _pair(args, k41_ranks=4, form=0, **opt):
     import oracle as O
     from spns_b200.hit import HIT
-    gpu = HIT(args, k41_ranks=k41_ranks, **opt)
+    gpu = HIT(args, k41_ranks=k41_ranks, nonlinear_form=form, **opt)
     ref = O.OracleHIT(args, k41_ranks=k41_ranks, **opt)
     return gpu, ref
 
@@ -36,14 +36,16 @@ def test_k41_initial_field_matches():
     assert abs(gpu.getEk_init() - ref.getEk_init()) <= 1e-13 * ref.getEk_init()
 
 
+@pytest.mark.parametrize("form", [0, 2], ids=["rotational+edge", "advective"])
 @pytest.mark.parametrize("opts", [
     dict(),
     dict(rotating=(1.5, -2.1, 3.0)),
     dict(self_adaptive=True),
     dict(conj=True),
 ])
-def test_dns_10_steps_n32(opts):
-    gpu, ref = _pair(make_args(32, nu=3.283e-4, **opts))
+def test_dns_10_steps_n32(opts, form):
+    """K41 field: the +-N/2 modes fill during the steps, so both forms must be exact there."""
+    gpu, ref = _pair(make_args(32, nu=3.283e-4, **opts), form=form)
     _run(gpu, ref, 10, check_each=True)
     assert rel_l2(gpu.get_compact(), ref.get_compact()) < TOL
     assert abs(gpu.gettime() - ref.gettime()) <= 1e-13 * ref.gettime()
@@ -93,6 +95,14 @@ def test_rotational_form_matches_when_edge_modes_are_empty():
     assert rel_l2(gpu.get_compact(), ref.get_compact()) < TOL
 
 
+def test_unsupported_grid_is_reported():
+    """Odd N gives M=(3N)/2 with no factor 3 (e.g. 46): outside the compiled FFT lengths."""
+    from spns_b200.hit import HIT, SpnsError
+    with pytest.raises(SpnsError) as ei:
+        HIT(make_args(31, nu=3.283e-4), k41_ranks=4)
+    assert ei.value.status == -2
+
+
 def test_les_10_steps_n32():
     gpu, ref = _pair(make_args(32, nu=3.283e-4, les=0.16))
     _run(gpu, ref, 10, check_each=True)
@@ -106,10 +116,11 @@ def test_les_rotating_noncubic():
     assert rel_l2(gpu.get_compact(), oracle_compact_to_true(ref.get_compact(), args)) < TOL
 
 
-def test_noncubic_true_grid():
+@pytest.mark.parametrize("form", [0, 2], ids=["rotational+edge", "advective"])
+def test_noncubic_true_grid(form):
     """Length factors (6,3,2): GPU runs the 48^3 true grid, the oracle the expanded 288x144x96 one."""
     args = make_args(32, nu=3.283e-4, L=(6, 3, 2))
-    gpu, ref = _pair(args)
+    gpu, ref = _pair(args, form=form)
     assert gpu.physical_shape[1:] == (48, 48, 48)
     assert rel_l2(gpu.get_compact(), oracle_compact_to_true(ref.get_compact(), args)) < 1e-14
     _run(gpu, ref, 3)
