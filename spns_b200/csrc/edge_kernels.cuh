@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(P *(L / E)) k_lines(cx<T> *__restrict__ data, 
     cx<T> r[E];
 #pragma unroll
     for (int e = 0; e < E; e++) r[e] = ok ? d[in_row<L, E, INV>(q, e)] : zero<T>();
-    fft<T, L, E, INV>(r, sm, q, tw);
+    fft<T, L, E, INV, SmPencil<T, L>, (32 % (L / E) == 0)>(r, sm, q, tw);
     if (ok)
 #pragma unroll
         for (int e = 0; e < E; e++) d[out_row<L, E, INV>(q, e)] = r[e];

@@ -3,17 +3,23 @@
 // One pencil of length L is processed by Q = L/E threads, each holding E
 // complex values in registers.  A stage of radix R performs E/R butterflies
 // per thread; between stages the values are exchanged through shared memory
-// (one buffer, two barriers per stage).  The first stage reads its inputs from
-// registers filled by the caller at rows  j + r*(L/R_first)  and the last stage
-// leaves its outputs in registers at rows  j + r*(L/R_last)  (j = q + Q*m), so
-// callers load pencils straight from global memory and store results straight
-// back (or keep them in registers for fused pointwise work).
+// (one buffer, two barriers per stage; warp barriers when a pencil lives in
+// one warp).  The first stage reads its inputs from registers filled by the
+// caller at rows  j + r*(L/R_first)  and the last stage leaves its outputs in
+// registers at rows  j + r*(L/R_last)  (j = q + Q*m), so callers load pencils
+// straight from global memory and store results straight back (or keep them
+// in registers for fused pointwise work).
 //
 // Stockham autosort, stage (R, Ns): butterfly j, k = j mod Ns,
 //   inputs  x_r = in[j + r*L/R],  x_r *= w_L^{r*k*L/(Ns*R)},  y = DFT_R(x),
 //   outputs out[(j/Ns)*Ns*R + k + r*Ns] = y_r.
-// Twiddles come from a table w_L^m = exp(-2*pi*i*m/L) computed on the host in
-// extended precision (the inverse uses the conjugate).
+// Radices 2, 3, 4, 6, 8, 12: the composite ones with a factor 3 use the
+// prime-factor (Good-Thomas) split 2x3 / 4x3, which needs no inner twiddles.
+// Twiddles: w^1 of a butterfly is read from a table w_L^m = exp(-2 pi i m/L)
+// computed on the host in extended precision; its powers w^r are formed by
+// repeated complex multiplication (one table read per butterfly instead of
+// R-1: the table reads contend with the shared-memory exchange for the
+// load/store pipe).  The inverse uses the conjugates.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -34,16 +40,18 @@ template <typename T> __device__ __forceinline__ cx<T> mul_i(cx<T> a) { return m
 template <typename T> __device__ __forceinline__ cx<T> zero() { return mk<T>(T(0), T(0)); }
 
 // ---------------------------------------------------------------------------
-// Radix plan: greedy factors of L, each dividing E (8, 4, 2, then 3).
-// Forward order = greedy order, inverse order = reversed greedy order, so the
-// last radix of an inverse transform equals the first radix of a forward one
-// (register hand-off between them needs the same row mapping).
+// Radix plan: greedy factors of L from {12, 8, 6, 4, 3, 2}, each dividing E.
+// Forward order = greedy order, inverse order = reversed, so the last radix of
+// an inverse transform equals the first radix of a forward one (the register
+// hand-off between them needs the same row mapping).
 // ---------------------------------------------------------------------------
 __host__ __device__ constexpr int pick_radix(int rem, int E) {
-    return (rem % 8 == 0 && E % 8 == 0) ? 8
+    return (rem % 12 == 0 && E % 12 == 0) ? 12
+         : (rem % 8 == 0 && E % 8 == 0) ? 8
+         : (rem % 6 == 0 && E % 6 == 0) ? 6
          : (rem % 4 == 0 && E % 4 == 0) ? 4
-         : (rem % 2 == 0 && E % 2 == 0) ? 2
-         : (rem % 3 == 0 && E % 3 == 0) ? 3 : 0;
+         : (rem % 3 == 0 && E % 3 == 0) ? 3
+         : (rem % 2 == 0 && E % 2 == 0) ? 2 : 0;
 }
 __host__ __device__ constexpr int n_stages(int L, int E) {
     int n = 0, rem = L;
@@ -100,19 +108,62 @@ template <typename T, bool INV> __device__ __forceinline__ void dft8(cx<T> *x) {
     x[2] = e[2] + o2;   x[6] = e[2] - o2;
     x[3] = e[3] + o3;   x[7] = e[3] - o3;
 }
+// Good-Thomas split of R = A*B (gcd 1): input n = (B a + A b) mod R, output
+// k with k = ka (mod A), k = kb (mod B); DFT_A over a, then DFT_B over b.
+template <int A, int B> struct PFA {
+    static constexpr int R = A * B;
+    __host__ __device__ static constexpr int in(int a, int b) { return (B * a + A * b) % R; }
+    __host__ __device__ static constexpr int out(int ka, int kb) {
+        int invB = 1;
+        while ((B * invB) % A != 1 % A) invB++;
+        int invA = 1;
+        while ((A * invA) % B != 1 % B) invA++;
+        return (ka * B * invB + kb * A * invA) % R;
+    }
+};
+template <typename T, bool INV, int A, int B> __device__ __forceinline__ void dft_pfa(cx<T> *x) {
+    using P = PFA<A, B>;
+    cx<T> t[A * B];
+#pragma unroll
+    for (int b = 0; b < B; b++) {
+        cx<T> col[A];
+#pragma unroll
+        for (int a = 0; a < A; a++) col[a] = x[P::in(a, b)];
+        if constexpr (A == 2) dft2<T, INV>(col);
+        else if constexpr (A == 4) dft4<T, INV>(col);
+        else dft8<T, INV>(col);
+#pragma unroll
+        for (int a = 0; a < A; a++) t[a * B + b] = col[a];
+    }
+#pragma unroll
+    for (int ka = 0; ka < A; ka++) {
+        cx<T> row[B];
+#pragma unroll
+        for (int b = 0; b < B; b++) row[b] = t[ka * B + b];
+        dft3<T, INV>(row);
+#pragma unroll
+        for (int kb = 0; kb < B; kb++) x[P::out(ka, kb)] = row[kb];
+    }
+}
 template <typename T, int R, bool INV> __device__ __forceinline__ void dft(cx<T> *x) {
     if constexpr (R == 2) dft2<T, INV>(x);
     else if constexpr (R == 3) dft3<T, INV>(x);
     else if constexpr (R == 4) dft4<T, INV>(x);
+    else if constexpr (R == 6) dft_pfa<T, INV, 2, 3>(x);
     else if constexpr (R == 8) dft8<T, INV>(x);
+    else if constexpr (R == 12) dft_pfa<T, INV, 4, 3>(x);
 }
 
 // ---------------------------------------------------------------------------
 // Stage engine.  SM is a shared-memory accessor:  cx<T>& SM::at(int row).
 // v[m*R + r] holds the input (before the stage) / output (after) of butterfly
-// j = q + Q*m, leg r.
+// j = q + Q*m, leg r.  WARP: the threads of a pencil exchange within one warp.
 // ---------------------------------------------------------------------------
-template <typename T, int L, int E, bool INV, int S, class SM>
+template <bool WARP> __device__ __forceinline__ void stage_barrier() {
+    if constexpr (WARP) __syncwarp(); else __syncthreads();
+}
+
+template <typename T, int L, int E, bool INV, bool WARP, int S, class SM>
 __device__ __forceinline__ void fft_run(cx<T> (&v)[E], SM sm, int q, const cx<T> *__restrict__ tw) {
     using PL = Plan<L, E, INV>;
     constexpr int R = PL::radix(S);
@@ -124,10 +175,12 @@ __device__ __forceinline__ void fft_run(cx<T> (&v)[E], SM sm, int q, const cx<T>
         if constexpr (Ns > 1) {
             const int j = q + Q * m;
             const int k = j % Ns;
+            const cx<T> w1 = tw[k * (L / (Ns * R))];
+            cx<T> w = w1;
 #pragma unroll
             for (int r = 1; r < R; r++) {
-                const cx<T> w = tw[r * k * (L / (Ns * R))];
                 v[m * R + r] = INV ? cmulc(v[m * R + r], w) : cmul(v[m * R + r], w);
+                if (r + 1 < R) w = cmul(w, w1);
             }
         }
         dft<T, R, INV>(&v[m * R]);
@@ -140,7 +193,7 @@ __device__ __forceinline__ void fft_run(cx<T> (&v)[E], SM sm, int q, const cx<T>
 #pragma unroll
             for (int r = 0; r < R; r++) sm.at(base + r * Ns) = v[m * R + r];
         }
-        __syncthreads();
+        stage_barrier<WARP>();
         constexpr int R2 = PL::radix(S + 1);
         constexpr int MB2 = E / R2;
 #pragma unroll
@@ -149,8 +202,8 @@ __device__ __forceinline__ void fft_run(cx<T> (&v)[E], SM sm, int q, const cx<T>
 #pragma unroll
             for (int r = 0; r < R2; r++) v[m * R2 + r] = sm.at(j + r * (L / R2));
         }
-        __syncthreads();
-        fft_run<T, L, E, INV, S + 1, SM>(v, sm, q, tw);
+        stage_barrier<WARP>();
+        fft_run<T, L, E, INV, WARP, S + 1, SM>(v, sm, q, tw);
     }
 }
 
@@ -169,11 +222,13 @@ template <int L, int E, bool INV> __device__ __forceinline__ int out_row(int q, 
 // The thread index goes through an opaque move so that the shared-memory
 // addresses of the stages are recomputed per transform instead of being kept
 // live across every transform of a kernel (which exhausts the register file).
-template <typename T, int L, int E, bool INV, class SM>
+// WARP=true only where each pencil's threads lie in one warp (Q divides 32 in a
+// pencil-major thread layout).
+template <typename T, int L, int E, bool INV, class SM, bool WARP = false>
 __device__ __forceinline__ void fft(cx<T> (&v)[E], SM sm, int q, const cx<T> *__restrict__ tw) {
     int qq;
     asm volatile("mov.b32 %0, %1;" : "=r"(qq) : "r"(q));
-    fft_run<T, L, E, INV, 0, SM>(v, sm, qq, tw);
+    fft_run<T, L, E, INV, WARP, 0, SM>(v, sm, qq, tw);
 }
 
 // Accessor: tile of P pencils stored row-major [row][P] (pencil index fastest).

@@ -255,7 +255,7 @@ template <typename T, int L, int E>
 __device__ __forceinline__ void k3_store_pair(cx<T> (&r)[E], SmPencil<T, L> sm, int q, int Kz, cx<T> *A, cx<T> *B,
                                               bool fold_dz_b_into_a, T sz, bool ok, const cx<T> *__restrict__ tw) {
     constexpr int Q = L / E;
-    fft<T, L, E, false>(r, sm, q, tw);
+    fft<T, L, E, false, SmPencil<T, L>, (32 % (L / E) == 0)>(r, sm, q, tw);
 #pragma unroll
     for (int e = 0; e < E; e++) sm.at(out_row<L, E, false>(q, e)) = r[e];
     __syncthreads();
@@ -277,7 +277,7 @@ __device__ __forceinline__ void k3_store_pair(cx<T> (&r)[E], SmPencil<T, L> sm, 
 template <typename T, int L, int E>
 __device__ __forceinline__ void k3_store_single(cx<T> (&r)[E], SmPencil<T, L> sm, int q, int Kz, cx<T> *A, bool ok,
                                                 const cx<T> *__restrict__ tw) {
-    fft<T, L, E, false>(r, sm, q, tw);
+    fft<T, L, E, false, SmPencil<T, L>, (32 % (L / E) == 0)>(r, sm, q, tw);
     if (ok) {
 #pragma unroll
         for (int e = 0; e < E; e++) {
@@ -324,9 +324,9 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
     if constexpr (MODE == MODE_VEL) {
         cx<T> A[E], B[E];
         k3_load_pair<T, L, E>(A, F(0), false, F(1), false, g.Kz, sz, q, ok);
-        fft<T, L, E, true>(A, sm, q, tw);
+        fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(A, sm, q, tw);
         k3_load_pair<T, L, E>(B, F(2), false, nullptr, false, g.Kz, sz, q, ok);
-        fft<T, L, E, true>(B, sm, q, tw);
+        fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(B, sm, q, tw);
         double ss = 0.0;
 #pragma unroll
         for (int e = 0; e < E; e++) {
@@ -351,11 +351,11 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
         // pairs (u, w_x), (v, w_y), (w, w_z);  c = w x u  (= u.grad u + gradient)
         cx<T> A[E], B[E], C[E];
         k3_load_pair<T, L, E>(A, F(0), false, F(3), false, g.Kz, sz, q, ok);
-        fft<T, L, E, true>(A, sm, q, tw);
+        fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(A, sm, q, tw);
         k3_load_pair<T, L, E>(B, F(1), false, F(4), false, g.Kz, sz, q, ok);
-        fft<T, L, E, true>(B, sm, q, tw);
+        fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(B, sm, q, tw);
         k3_load_pair<T, L, E>(C, F(2), false, F(5), false, g.Kz, sz, q, ok);
-        fft<T, L, E, true>(C, sm, q, tw);
+        fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(C, sm, q, tw);
 #pragma unroll
         for (int e = 0; e < E; e++) {
             const T uu = A[e].x, ox = A[e].y, vv = B[e].x, oy = B[e].y, ww = C[e].x, oz = C[e].y;
@@ -377,12 +377,12 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
 #define PH(slot, row) ph[(slot) * L + (row)]
         // (u, v)
         k3_load_pair<T, L, E>(A, F(0), false, F(1), false, g.Kz, sz, q, ok);
-        fft<T, L, E, true>(A, sm, q, tw);
+        fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(A, sm, q, tw);
 #pragma unroll
         for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); PH(0, row) = A[e].x; PH(1, row) = A[e].y; }
         // (w, du/dz)
         k3_load_pair<T, L, E>(A, F(2), false, F(0), true, g.Kz, sz, q, ok);
-        fft<T, L, E, true>(A, sm, q, tw);
+        fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(A, sm, q, tw);
 #pragma unroll
         for (int e = 0; e < E; e++) {
             const int row = out_row<L, E, true>(q, e);
@@ -394,7 +394,7 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
         }
         // (du/dx, du/dy)
         k3_load_pair<T, L, E>(A, F(3), false, F(6), false, g.Kz, sz, q, ok);
-        fft<T, L, E, true>(A, sm, q, tw);
+        fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(A, sm, q, tw);
 #pragma unroll
         for (int e = 0; e < E; e++) {
             const int row = out_row<L, E, true>(q, e);
@@ -403,7 +403,7 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
         }
         // (dv/dx, dv/dy)
         k3_load_pair<T, L, E>(A, F(4), false, F(7), false, g.Kz, sz, q, ok);
-        fft<T, L, E, true>(A, sm, q, tw);
+        fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(A, sm, q, tw);
 #pragma unroll
         for (int e = 0; e < E; e++) {
             const int row = out_row<L, E, true>(q, e);
@@ -412,7 +412,7 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
         }
         // (dw/dx, dw/dy)
         k3_load_pair<T, L, E>(A, F(5), false, F(8), false, g.Kz, sz, q, ok);
-        fft<T, L, E, true>(A, sm, q, tw);
+        fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(A, sm, q, tw);
 #pragma unroll
         for (int e = 0; e < E; e++) {
             const int row = out_row<L, E, true>(q, e);
@@ -421,7 +421,7 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
         }
         // (dv/dz, dw/dz)
         k3_load_pair<T, L, E>(A, F(1), true, F(2), true, g.Kz, sz, q, ok);
-        fft<T, L, E, true>(A, sm, q, tw);
+        fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(A, sm, q, tw);
 #pragma unroll
         for (int e = 0; e < E; e++) {
             const int row = out_row<L, E, true>(q, e);

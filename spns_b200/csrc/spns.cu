@@ -31,24 +31,39 @@ static bool length_supported(int L) {
     return false;
 }
 
-template <typename T, int L> struct Shape {
-    static constexpr int E = 12;             // complex values per thread
+// Tile shapes per pass (complex values per thread E, threads per block),
+// chosen by timing the N=512 step on B200.
+template <typename T, int L, int E_, int THR> struct ShapeT {
+    static constexpr int E = E_;             // complex values per thread
     static constexpr int Q = L / E;          // threads per pencil
-    static constexpr int P0 = 256 / Q;
+    static constexpr int P0 = THR / Q;
     static constexpr int P = P0 >= 32 ? 32 : P0 >= 16 ? 16 : P0 >= 8 ? 8 : 4; // pencils per block
     static constexpr int THREADS = P * Q;
     static constexpr size_t SMEM_ROW = (size_t)L * P * sizeof(cx<T>);
     static constexpr size_t SMEM_PEN = (size_t)SmPencil<T, L>::PITCH * P * sizeof(cx<T>);
 };
+template <typename T, int L> using ShapeK1 = ShapeT<T, L, 12, 256>;   // inverse x
+template <typename T, int L> using ShapeK2 = ShapeT<T, L, 24, 256>;   // inverse y (and forward y)
+template <typename T, int L> using ShapeK5 = ShapeT<T, L, 24, 128>;   // forward x
+template <typename T, int L> using Shape = ShapeT<T, L, 24, 128>;     // edge planes, test lines
+#ifndef SPNS_Z_THREADS
+#define SPNS_Z_THREADS 128    // threads per block in the z pass (2 blocks per SM)
+#endif
+#ifndef SPNS_Z_E
+#define SPNS_Z_E 12           // complex values per thread in the z pass (3 pairs in registers)
+#endif
 
 // z pass: pencils per block limited by the shared memory of the exchange
 // buffer plus the physical fields kept per pencil.
 template <typename T, int L, int MODE> struct Shape3 {
-    using S = Shape<T, L>;
+    static constexpr int E = SPNS_Z_E;       // the z pass keeps several fields in registers
+    static constexpr int Q = L / E;
+    static constexpr int ZT = SPNS_Z_THREADS / Q;
+    static constexpr int P0 = ZT >= 32 ? 32 : ZT >= 16 ? 16 : ZT >= 8 ? 8 : ZT >= 4 ? 4 : ZT >= 2 ? 2 : 1;
     static constexpr size_t PER_PEN = (size_t)SmPencil<T, L>::PITCH * sizeof(cx<T>) + (size_t)K3Phys<MODE>::N * L * sizeof(T);
     static constexpr int PMAX = (int)((200 * 1024) / PER_PEN);
-    static constexpr int P = S::P <= PMAX ? S::P : PMAX >= 16 ? 16 : PMAX >= 8 ? 8 : PMAX >= 4 ? 4 : PMAX >= 2 ? 2 : 1;
-    static constexpr int THREADS = P * S::Q;
+    static constexpr int P = P0 <= PMAX ? P0 : PMAX >= 16 ? 16 : PMAX >= 8 ? 8 : PMAX >= 4 ? 4 : PMAX >= 2 ? 2 : 1;
+    static constexpr int THREADS = P * Q;
     static constexpr size_t SMEM = PER_PEN * P;
 };
 
@@ -75,6 +90,10 @@ struct spns_handle {
     std::map<int, double2 *> tw;                     // twiddle tables per length
     std::string err;
     int kernels_per_step = 0;
+    // CUDA graphs of one step, per parity of the state-buffer swap (kappa scheme)
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    double2 *U0 = nullptr;                           // state buffer of parity 0
+    bool use_graphs = true;
     // optional per-kernel event profile of the next steps (spns_profile_*)
     std::vector<cudaEvent_t> prof_ev;
     std::vector<std::string> prof_names;
@@ -137,7 +156,7 @@ template <class K> static cudaError_t set_smem(K kern, size_t bytes) {
 using T64 = double;
 
 template <int L, int MODE> static cudaError_t launch_k1(spns_handle *h) {
-    using S = Shape<T64, L>;
+    using S = ShapeK1<T64, L>;
     auto kern = k1_inv_x<T64, L, S::E, S::P, MODE>;
     cudaError_t e = set_smem(kern, S::SMEM_ROW);
     if (e != cudaSuccess) return e;
@@ -148,7 +167,7 @@ template <int L, int MODE> static cudaError_t launch_k1(spns_handle *h) {
     return cudaGetLastError();
 }
 template <int L, int MODE> static cudaError_t launch_k2(spns_handle *h) {
-    using S = Shape<T64, L>;
+    using S = ShapeK2<T64, L>;
     auto kern = k2_inv_y<T64, L, S::E, S::P, MODE>;
     cudaError_t e = set_smem(kern, S::SMEM_ROW);
     if (e != cudaSuccess) return e;
@@ -157,9 +176,8 @@ template <int L, int MODE> static cudaError_t launch_k2(spns_handle *h) {
     return cudaGetLastError();
 }
 template <int L, int MODE> static cudaError_t launch_k3(spns_handle *h, double *phys) {
-    using S = Shape<T64, L>;
     using S3 = Shape3<T64, L, MODE>;
-    auto kern = k3_z<T64, L, S::E, S3::P, MODE>;
+    auto kern = k3_z<T64, L, S3::E, S3::P, MODE>;
     cudaError_t e = set_smem(kern, S3::SMEM);
     if (e != cudaSuccess) return e;
     const long long npen = (long long)h->g.Mx * h->g.My;
@@ -168,7 +186,7 @@ template <int L, int MODE> static cudaError_t launch_k3(spns_handle *h, double *
     return cudaGetLastError();
 }
 template <int L, int MODE> static cudaError_t launch_k4(spns_handle *h) {
-    using S = Shape<T64, L>;
+    using S = ShapeK2<T64, L>;
     auto kern = k4_fwd_y<T64, L, S::E, S::P, MODE>;
     cudaError_t e = set_smem(kern, S::SMEM_ROW);
     if (e != cudaSuccess) return e;
@@ -177,7 +195,7 @@ template <int L, int MODE> static cudaError_t launch_k4(spns_handle *h) {
     return cudaGetLastError();
 }
 template <int L, int MODE> static cudaError_t launch_k5(spns_handle *h) {
-    using S = Shape<T64, L>;
+    using S = ShapeK5<T64, L>;
     auto kern = k5_fwd_x<T64, L, S::E, S::P, MODE>;
     cudaError_t e = set_smem(kern, S::SMEM_ROW);
     if (e != cudaSuccess) return e;
@@ -541,6 +559,7 @@ static void free_handle(spns_handle *h) {
     cudaFree(h->bins); cudaFree(h->FT); cudaFree(h->forced); cudaFree(h->phys); cudaFree(h->edge);
     for (auto &kv : h->tw) cudaFree(kv.second);
     for (auto ev : h->prof_ev) cudaEventDestroy(ev);
+    for (auto &gx : h->graph) if (gx) cudaGraphExecDestroy(gx);
     if (h->st) cudaStreamDestroy(h->st);
     delete h;
 }
@@ -680,6 +699,11 @@ int spns_create(const spns_hit_args *args, const double *file_uvw, spns_handle *
         rc = forcing_energy_cascade(h, K41.data(), h->last_rad, 0);
         if (rc) { g_create_error = h->err; return cleanup(rc); }
     }
+    h->U0 = h->U;
+    {
+        const char *ng = getenv("SPNS_NO_GRAPHS");
+        h->use_graphs = !(ng && ng[0] == '1');
+    }
     rc = run_velocity(h, nullptr);
     if (rc) { g_create_error = h->err; return cleanup(rc); }
     if (!a.isReLambda) {
@@ -703,10 +727,36 @@ int spns_destroy(spns_handle *h) {
     return SPNS_OK;
 }
 
+// One step as a replay of a captured CUDA graph.  The kernel arguments hold
+// the state-buffer pointers, which the kappa scheme swaps every step, so one
+// graph is kept per parity.  Capture issues no work; the first (uncaptured)
+// step of a handle sets the kernels' attributes before any capture.
+static int step_graph(spns_handle *h) {
+    const int par = (h->U == h->U0) ? 0 : 1;
+    if (!h->graph[par]) {
+        double2 *U = h->U, *Up = h->Up;
+        cudaGraph_t gr = nullptr;
+        CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+        int r = step_once(h);
+        cudaError_t e = cudaStreamEndCapture(h->st, &gr);
+        h->U = U; h->Up = Up;
+        if (r) { if (gr) cudaGraphDestroy(gr); return r; }
+        if (e != cudaSuccess) return fail(h, SPNS_ERR_CUDA, "step capture failed: %s", cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&h->graph[par], gr, 0);
+        cudaGraphDestroy(gr);
+        if (e != cudaSuccess) return fail(h, SPNS_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(e));
+    }
+    CK(cudaGraphLaunch(h->graph[par], h->st));
+    if (h->a.isSelfAdaptive) std::swap(h->U, h->Up);
+    return SPNS_OK;
+}
+
 int spns_step(spns_handle *h, int nsteps) {
     if (!h || nsteps < 0) return SPNS_ERR_INVALID_ARGUMENT;
     for (int i = 0; i < nsteps; i++) {
-        int r = step_once(h);
+        const bool profiling = h->prof_steps < h->prof_cap_steps;
+        const bool warm = h->kernels_per_step > 0;   // a first step has run uncaptured
+        int r = (h->use_graphs && warm && !profiling) ? step_graph(h) : step_once(h);
         if (r) return r;
     }
     return check_flags(h);
@@ -940,14 +990,14 @@ __global__ void k_fft1d_lines(double2 *data, int batch, int sign, const double2 
     if (sign < 0) {
 #pragma unroll
         for (int e = 0; e < E; e++) r[e] = ok ? d[in_row<L, E, false>(q, e)] : zero<double>();
-        fft<double, L, E, false>(r, sm, q, (const cx<double> *)tw);
+        fft<double, L, E, false, SmPencil<double, L>, (32 % (L / E) == 0)>(r, sm, q, (const cx<double> *)tw);
         if (ok)
 #pragma unroll
             for (int e = 0; e < E; e++) d[out_row<L, E, false>(q, e)] = r[e];
     } else {
 #pragma unroll
         for (int e = 0; e < E; e++) r[e] = ok ? d[in_row<L, E, true>(q, e)] : zero<double>();
-        fft<double, L, E, true>(r, sm, q, (const cx<double> *)tw);
+        fft<double, L, E, true, SmPencil<double, L>, (32 % (L / E) == 0)>(r, sm, q, (const cx<double> *)tw);
         if (ok)
 #pragma unroll
             for (int e = 0; e < E; e++) d[out_row<L, E, true>(q, e)] = r[e];

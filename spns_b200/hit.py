@@ -16,7 +16,7 @@ import numpy as np
 from .params import HitArgs
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "_lib", "libspns.so")
+LIB_PATH = os.environ.get("SPNS_LIB", os.path.join(_HERE, "_lib", "libspns.so"))
 
 SPNS_FP64 = 0
 SPNS_FP32_HILO = 1
