@@ -240,6 +240,7 @@ def run_gpu(args):
     torch.cuda.set_device(local)
     from spns_b200.hit import HIT
     from spns_b200.fields import seeded_spectral_field
+    from spns_b200.replicas import whole_job_rate
 
     N = args.n
     a = box_args(N, nxy=args.nxy)
@@ -267,6 +268,7 @@ def run_gpu(args):
     barrier(dist)
     ms = ev0.elapsed_time(ev1)
     ms_max = reduce_max(dist, ms)
+    ek64 = h.Recalculate_Energy_Cascade()       # spectrum after W + K steps (FP32 comparison below)
 
     # --- per-kernel breakdown: the same K steps again, uncaptured, with an event before every kernel ---
     h.profile_begin(args.steps)
@@ -288,11 +290,43 @@ def run_gpu(args):
     finite = math.isfinite(s.Ek_Tot) and math.isfinite(s.At)
     h.close()
 
+    # --- compensated FP32 form on the same initial state: same W + K steps, timed the same way ---
+    fp32 = None
+    if not args.no_fp32:
+        from spns_b200.hit import SPNS_FP32_HILO
+        h32 = HIT(a, device=local, eps_forcing=EPS, precision=SPNS_FP32_HILO)
+        U0 = seeded_spectral_field(a.Nx, a.Ny, a.Nz, kp=KP, seed=SEED + rank)
+        h32.set_compact(U0)
+        del U0
+        h32.Recalculate_Velocity_Antitransform()
+        h32.Recalculate_TimeStep()
+        s32 = torch.cuda.ExternalStream(h32.stream_handle(), device=torch.device("cuda", local))
+        for _ in range(args.warmup):
+            h32.New_Fractional_Step_Method()
+        barrier(dist)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s32)
+        h32._ck(h32._L.spns_step(h32._h, args.steps))
+        e1.record(s32)
+        torch.cuda.synchronize()
+        barrier(dist)
+        ms32_max = reduce_max(dist, e0.elapsed_time(e1))
+        ek32 = h32.Recalculate_Energy_Cascade()
+        h32.close()
+        mask = ek64 > 1e-6 * ek64.max()
+        fp32 = {"value": whole_job_rate(world, args.steps, ms32_max / 1e3), "unit": "steps/s",
+                "ms_per_step": ms32_max / args.steps, "speedup_vs_fp64": ms_max / ms32_max,
+                "dtype": "f32 transforms and products, f32 hi+lo state (~48 bits), f64 reductions/CFL/forcing",
+                "ek_max_shell_rel_err_vs_fp64": float(np.max(np.abs(ek32[mask] - ek64[mask]) / ek64[mask])),
+                "ek_max_abs_err_over_ek_tot": float(np.max(np.abs(ek32 - ek64)) / ek64.sum()),
+                "steps_compared": args.warmup + args.steps,
+                "shells_compared": "shells holding more than 1e-6 of the peak shell energy"}
+
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
         return 0
-    from spns_b200.replicas import whole_job_rate
     value = whole_job_rate(world, args.steps, ms_max / 1e3)
     e2e_value = whole_job_rate(world, args.steps, e2e_max)
     # roofline of the dominant kernel
@@ -330,6 +364,7 @@ def run_gpu(args):
         "graphs": "timed steps replay one CUDA graph per step",
         "step_algorithmic_bytes": step_bytes,
         "step_achieved_GBps": step_bytes / (ms_max / args.steps / 1e3) / 1e9,
+        "fp32_hilo": fp32,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                      "algorithmic_bytes": bytes_per[dom]},
@@ -354,6 +389,7 @@ def main():
                          "that runs the same z-pass kernel, for profiling")
     ap.add_argument("--ref-sample-n", type=int, default=96)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp32", action="store_true", help="skip the compensated FP32 form's extra line field")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

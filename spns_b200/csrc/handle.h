@@ -1,0 +1,206 @@
+// handle.h -- the solver handle of libspns and the launch machinery shared by
+// the translation units (spns.cu: C ABI; spns_f64.cu / spns_f32.cu: the passes
+// of one step instantiated for one precision).
+#pragma once
+#include "spns.h"
+#include "solver_kernels.cuh"
+#include "edge_kernels.cuh"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <map>
+#include <string>
+#include <vector>
+
+// ---------------------------------------------------------------------------
+// Compiled FFT lengths and launch shapes
+// ---------------------------------------------------------------------------
+#define SPNS_FOR_EACH_LENGTH(X) X(48) X(72) X(96) X(144) X(192) X(288) X(384) X(768) X(1536)
+
+inline bool spns_length_supported(int L) {
+#define SPNS_CASE(n) if (L == n) return true;
+    SPNS_FOR_EACH_LENGTH(SPNS_CASE)
+#undef SPNS_CASE
+    return false;
+}
+
+// Tile shapes per pass (complex values per thread E, threads per block),
+// chosen by timing the N=512 step on B200.
+template <typename T, int L, int E_, int THR> struct ShapeT {
+    static constexpr int E = E_;             // complex values per thread
+    static constexpr int Q = L / E;          // threads per pencil
+    static constexpr int P0 = THR / Q;
+    static constexpr int P = P0 >= 32 ? 32 : P0 >= 16 ? 16 : P0 >= 8 ? 8 : 4; // pencils per block
+    static constexpr int THREADS = P * Q;
+    static constexpr size_t SMEM_ROW = (size_t)L * P * sizeof(spns::cx<T>);
+    static constexpr size_t SMEM_PEN = (size_t)spns::SmPencil<T, L>::PITCH * P * sizeof(spns::cx<T>);
+};
+// Double precision shapes (E, threads per block); single precision has its own
+// (half the register and shared-memory footprint per value).
+#ifndef SPNS_F32_K1_E
+#define SPNS_F32_K1_E 12
+#endif
+#ifndef SPNS_F32_K1_T
+#define SPNS_F32_K1_T 256
+#endif
+#ifndef SPNS_F32_K2_E
+#define SPNS_F32_K2_E 24
+#endif
+#ifndef SPNS_F32_K2_T
+#define SPNS_F32_K2_T 512
+#endif
+#ifndef SPNS_F32_K5_E
+#define SPNS_F32_K5_E 24
+#endif
+#ifndef SPNS_F32_K5_T
+#define SPNS_F32_K5_T 256
+#endif
+#ifndef SPNS_F32_Z_E
+#define SPNS_F32_Z_E 12
+#endif
+#ifndef SPNS_F32_Z_T
+#define SPNS_F32_Z_T 256
+#endif
+#ifndef SPNS_Z_THREADS
+#define SPNS_Z_THREADS 128    // threads per block in the double z pass (2 blocks per SM)
+#endif
+#ifndef SPNS_Z_E
+#define SPNS_Z_E 12           // complex values per thread in the double z pass (3 pairs in registers)
+#endif
+template <typename T> struct ShapeSel {
+    static constexpr bool D = sizeof(T) == 8;
+    static constexpr int K1_E = D ? 12 : SPNS_F32_K1_E, K1_T = D ? 256 : SPNS_F32_K1_T;
+    static constexpr int K2_E = D ? 24 : SPNS_F32_K2_E, K2_T = D ? 256 : SPNS_F32_K2_T;
+    static constexpr int K5_E = D ? 24 : SPNS_F32_K5_E, K5_T = D ? 128 : SPNS_F32_K5_T;
+    static constexpr int Z_E = D ? SPNS_Z_E : SPNS_F32_Z_E, Z_T = D ? SPNS_Z_THREADS : SPNS_F32_Z_T;
+};
+template <typename T, int L> using ShapeK1 = ShapeT<T, L, ShapeSel<T>::K1_E, ShapeSel<T>::K1_T>;   // inverse x
+template <typename T, int L> using ShapeK2 = ShapeT<T, L, ShapeSel<T>::K2_E, ShapeSel<T>::K2_T>;   // inverse y (and forward y)
+template <typename T, int L> using ShapeK5 = ShapeT<T, L, ShapeSel<T>::K5_E, ShapeSel<T>::K5_T>;   // forward x
+template <typename T, int L> using Shape = ShapeT<T, L, 24, 128>;                                   // edge planes, test lines
+
+// z pass: pencils per block limited by the shared memory of the exchange
+// buffer plus the physical fields kept per pencil.
+template <typename T, int L, int MODE> struct Shape3 {
+    static constexpr int E = ShapeSel<T>::Z_E;   // the z pass keeps several fields in registers
+    static constexpr int Q = L / E;
+    static constexpr int ZT = ShapeSel<T>::Z_T / Q;
+    static constexpr int P0 = ZT >= 32 ? 32 : ZT >= 16 ? 16 : ZT >= 8 ? 8 : ZT >= 4 ? 4 : ZT >= 2 ? 2 : 1;
+    static constexpr size_t PER_PEN = (size_t)spns::SmPencil<T, L>::PITCH * sizeof(spns::cx<T>) + (size_t)spns::K3Phys<MODE>::N * L * sizeof(T);
+    static constexpr int PMAX = (int)((200 * 1024) / PER_PEN);
+    static constexpr int P = P0 <= PMAX ? P0 : PMAX >= 16 ? 16 : PMAX >= 8 ? 8 : PMAX >= 4 ? 4 : PMAX >= 2 ? 2 : 1;
+    static constexpr int THREADS = P * Q;
+    static constexpr size_t SMEM = PER_PEN * P;
+};
+
+// ---------------------------------------------------------------------------
+// Handle
+// ---------------------------------------------------------------------------
+// Device buffers are typed by the precision of the handle: element cx<double>
+// (SPNS_FP64) or cx<float> (SPNS_FP32_HILO; the spectral state and the
+// kappa-scheme history then carry a low part Ulo/Uplo with u = hi + lo).
+struct spns_handle {
+    spns_hit_args a;
+    int prec = SPNS_FP64;
+    size_t csz = 16;                                 // bytes per complex element
+    spns::Geo g;
+    spns::StepConsts c;
+    int last_rad = 0, last_rad_max = 0;
+    double delta = 0, Ek_init = 0, Ek_init_file = 0, Enstrophy_init_file = 0;
+    cudaStream_t st = nullptr;
+    spns::DevScalars *ds = nullptr;
+    void *U = nullptr, *Ulo = nullptr;               // state u^n (3 fields of S0)
+    void *Up = nullptr, *Uplo = nullptr;             // u^{n-1} (kappa scheme)
+    void *R = nullptr;                               // R^{n-1}
+    void *B1 = nullptr, *B2 = nullptr;               // S1 and S2 work buffers
+    int nB1 = 0, nB2 = 0;
+    double *bins = nullptr;                          // Ek[0..Kmax], Om[0..Kmax]
+    double *FT = nullptr, *forced = nullptr;
+    int forced_cap = 0;
+    double *phys = nullptr;
+    void *edge = nullptr;                            // edge-correction planes (rotational form)
+    bool edge_axis[3] = {false, false, false};       // axes whose +-N/2 planes alias (M = 3h)
+    std::map<int, void *> tw;                        // twiddle tables per length (precision of the handle)
+    std::string err;
+    int kernels_per_step = 0;
+    // CUDA graphs of one step, per parity of the state-buffer swap (kappa scheme)
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    void *U0 = nullptr;                              // state buffer of parity 0
+    bool use_graphs = true;
+    // optional per-kernel event profile of the next steps (spns_profile_*)
+    std::vector<cudaEvent_t> prof_ev;
+    std::vector<std::string> prof_names;
+    int prof_cap_steps = 0, prof_steps = 0, prof_nk = 0;
+};
+
+// Records the error text (handle, or the handle-less slot) and returns code.
+int spns_fail(spns_handle *h, int code, const char *fmt, ...);
+
+#define CK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return spns_fail(h, e_ == cudaErrorMemoryAllocation ? SPNS_ERR_OUT_OF_MEMORY : SPNS_ERR_CUDA, \
+                             "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+#define CKL()                                                                                      \
+    do {                                                                                           \
+        cudaError_t e_ = cudaGetLastError();                                                       \
+        if (e_ != cudaSuccess)                                                                     \
+            return spns_fail(h, SPNS_ERR_CUDA, "kernel launch failed: %s (%s:%d)", cudaGetErrorString(e_), \
+                             __FILE__, __LINE__);                                                  \
+    } while (0)
+
+#define LAUNCH(expr)                                                                              \
+    do {                                                                                          \
+        cudaError_t e_ = (expr);                                                                  \
+        if (e_ != cudaSuccess)                                                                    \
+            return spns_fail(h, SPNS_ERR_CUDA, "launch failed: %s (%s:%d)", cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+#define DISPATCH(Lval, call)                                                                 \
+    switch (Lval) {                                                                          \
+    case 48: { constexpr int LL = 48; call; } break;                                         \
+    case 72: { constexpr int LL = 72; call; } break;                                         \
+    case 96: { constexpr int LL = 96; call; } break;                                         \
+    case 144: { constexpr int LL = 144; call; } break;                                       \
+    case 192: { constexpr int LL = 192; call; } break;                                       \
+    case 288: { constexpr int LL = 288; call; } break;                                       \
+    case 384: { constexpr int LL = 384; call; } break;                                       \
+    case 768: { constexpr int LL = 768; call; } break;                                       \
+    case 1536: { constexpr int LL = 1536; call; } break;                                     \
+    default: return spns_fail(h, SPNS_ERR_UNSUPPORTED_SIZE, "FFT length %d is not compiled", Lval); \
+    }
+
+// Twiddle table w_L^m = exp(-2 pi i m / L), computed in extended precision.
+template <typename T> inline void *spns_make_twiddles(int L) {
+    std::vector<spns::cx<T>> t(L);
+    for (int m = 0; m < L; m++) {
+        long double ang = 2.0L * 3.14159265358979323846264338327950288L * (long double)m / (long double)L;
+        t[m].x = (T)cosl(ang);
+        t[m].y = (T)(-sinl(ang));
+    }
+    void *d = nullptr;
+    if (cudaMalloc(&d, sizeof(spns::cx<T>) * L) != cudaSuccess) return nullptr;
+    if (cudaMemcpy(d, t.data(), sizeof(spns::cx<T>) * L, cudaMemcpyHostToDevice) != cudaSuccess) { cudaFree(d); return nullptr; }
+    return d;
+}
+
+template <class K> inline cudaError_t spns_set_smem(K kern, size_t bytes) {
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+// Precision-specific operations of a handle (spns_f64.cu, spns_f32.cu).
+struct PrecOps {
+    int (*step_once)(spns_handle *h);                         // one New_Fractional_Step_Method
+    int (*run_velocity)(spns_handle *h, double *phys);        // inverse transform of u (CFL maxima)
+    int (*shell_sums)(spns_handle *h);                        // E(K), Om(K) of u into h->bins
+    int (*forcing_scale)(spns_handle *h, int last_eff, int nullify); // u *= FT[K]
+    int (*conj_correction)(spns_handle *h);                   // kz=0 conjugate correction
+};
+extern const PrecOps spns_ops_f64;
+extern const PrecOps spns_ops_f32;
+inline const PrecOps &spns_ops(const spns_handle *h) { return h->prec == SPNS_FP64 ? spns_ops_f64 : spns_ops_f32; }

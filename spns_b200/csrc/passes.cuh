@@ -1,0 +1,232 @@
+// passes.cuh -- launch code of one step, templated on the arithmetic type T of
+// the transforms (double: FP64 form; float: compensated FP32 hi/lo form).
+// Included by exactly one translation unit per precision (spns_f64.cu,
+// spns_f32.cu), which exports the PrecOps table of that precision.
+#pragma once
+#include "handle.h"
+
+#include <algorithm>
+
+template <typename T> struct Passes {
+    using C = spns::cx<T>;
+    static constexpr bool HILO = sizeof(T) == 4;
+
+    static C *U(spns_handle *h, int f = 0) { return (C *)h->U + (long long)f * h->g.S0; }
+    static C *Ulo(spns_handle *h, int f = 0) { return HILO ? (C *)h->Ulo + (long long)f * h->g.S0 : nullptr; }
+    static const C *tw(spns_handle *h, int L) { return (const C *)h->tw[L]; }
+
+    template <int L, int MODE> static cudaError_t launch_k1(spns_handle *h) {
+        using S = ShapeK1<T, L>;
+        auto kern = spns::k1_inv_x<T, L, S::E, S::P, MODE>;
+        cudaError_t e = spns_set_smem(kern, S::SMEM_ROW);
+        if (e != cudaSuccess) return e;
+        dim3 grid((h->g.Kz + S::P - 1) / S::P, h->g.Ky);
+        kern<<<grid, S::THREADS, S::SMEM_ROW, h->st>>>(h->g, U(h, 0), U(h, 1), U(h, 2), (C *)h->B1, tw(h, L));
+        return cudaGetLastError();
+    }
+    template <int L, int MODE> static cudaError_t launch_k2(spns_handle *h) {
+        using S = ShapeK2<T, L>;
+        auto kern = spns::k2_inv_y<T, L, S::E, S::P, MODE>;
+        cudaError_t e = spns_set_smem(kern, S::SMEM_ROW);
+        if (e != cudaSuccess) return e;
+        dim3 grid((h->g.Kz + S::P - 1) / S::P, h->g.Mx);
+        kern<<<grid, S::THREADS, S::SMEM_ROW, h->st>>>(h->g, (const C *)h->B1, (C *)h->B2, tw(h, L));
+        return cudaGetLastError();
+    }
+    template <int L, int MODE> static cudaError_t launch_k3(spns_handle *h, double *phys) {
+        using S3 = Shape3<T, L, MODE>;
+        auto kern = spns::k3_z<T, L, S3::E, S3::P, MODE>;
+        cudaError_t e = spns_set_smem(kern, S3::SMEM);
+        if (e != cudaSuccess) return e;
+        const long long npen = (long long)h->g.Mx * h->g.My;
+        dim3 grid((unsigned)((npen + S3::P - 1) / S3::P));
+        kern<<<grid, S3::THREADS, S3::SMEM, h->st>>>(h->g, (C *)h->B2, h->c, h->ds, phys, tw(h, L));
+        return cudaGetLastError();
+    }
+    template <int L, int MODE> static cudaError_t launch_k4(spns_handle *h) {
+        using S = ShapeK2<T, L>;
+        auto kern = spns::k4_fwd_y<T, L, S::E, S::P, MODE>;
+        cudaError_t e = spns_set_smem(kern, S::SMEM_ROW);
+        if (e != cudaSuccess) return e;
+        dim3 grid((h->g.Kz + S::P - 1) / S::P, h->g.Mx);
+        kern<<<grid, S::THREADS, S::SMEM_ROW, h->st>>>(h->g, (const C *)h->B2, (C *)h->B1, tw(h, L));
+        return cudaGetLastError();
+    }
+    template <int L, int MODE> static cudaError_t launch_k5(spns_handle *h) {
+        using S = ShapeK5<T, L>;
+        auto kern = spns::k5_fwd_x<T, L, S::E, S::P, MODE>;
+        cudaError_t e = spns_set_smem(kern, S::SMEM_ROW);
+        if (e != cudaSuccess) return e;
+        dim3 grid((h->g.Kz + S::P - 1) / S::P, h->g.Ky);
+        kern<<<grid, S::THREADS, S::SMEM_ROW, h->st>>>(h->g, (const C *)h->B1, (C *)h->B2, tw(h, L));
+        return cudaGetLastError();
+    }
+    // Spectral sweep; with the kappa scheme the new state goes into the u^{n-1}
+    // buffers and the state buffers are swapped after the launch.
+    static cudaError_t launch_k6(spns_handle *h) {
+        const int n = h->g.Kx * h->g.Kz;
+        dim3 grid((n + 255) / 256, h->g.Ky);
+        const C *G = (const C *)h->B2;
+        if (h->a.isSelfAdaptive) {
+            spns::k6_sweep<T, true><<<grid, 256, 0, h->st>>>(h->g, G, U(h), Ulo(h), (C *)h->R, (C *)h->Up, (C *)h->Uplo,
+                                                              (const C *)h->Up, (const C *)h->Uplo, h->c, h->ds);
+            std::swap(h->U, h->Up);
+            std::swap(h->Ulo, h->Uplo);
+        } else {
+            spns::k6_sweep<T, false><<<grid, 256, 0, h->st>>>(h->g, G, U(h), Ulo(h), (C *)h->R, U(h), Ulo(h), nullptr, nullptr,
+                                                               h->c, h->ds);
+        }
+        return cudaGetLastError();
+    }
+
+    // Batched 1-D FFTs for the 2-D edge planes.
+    template <int L, bool INV> static cudaError_t launch_lines(spns_handle *h, C *data, long long batch) {
+        using S = Shape<T, L>;
+        auto kern = spns::k_lines<T, L, S::E, S::P, INV>;
+        cudaError_t e = spns_set_smem(kern, S::SMEM_PEN);
+        if (e != cudaSuccess) return e;
+        kern<<<(unsigned)((batch + S::P - 1) / S::P), S::THREADS, S::SMEM_PEN, h->st>>>(data, batch, tw(h, L));
+        return cudaGetLastError();
+    }
+    template <int L, bool INV> static cudaError_t launch_cols(spns_handle *h, C *data, int ncols, int nbatch) {
+        using S = Shape<T, L>;
+        auto kern = spns::k_cols<T, L, S::E, S::P, INV>;
+        cudaError_t e = spns_set_smem(kern, S::SMEM_ROW);
+        if (e != cudaSuccess) return e;
+        dim3 grid((ncols + S::P - 1) / S::P, nbatch);
+        kern<<<grid, S::THREADS, S::SMEM_ROW, h->st>>>(data, ncols, tw(h, L));
+        return cudaGetLastError();
+    }
+
+    // Inverse transform of the velocity only (Recalculate_Velocity_Antitransform):
+    // refreshes the CFL maxima and, if phys != NULL, writes u,v,w on the grid.
+    static int run_velocity(spns_handle *h, double *phys) {
+        spns::k_reset_max<<<1, 1, 0, h->st>>>(h->ds);
+        CKL();
+        DISPATCH(h->g.Mx, LAUNCH((launch_k1<LL, spns::MODE_VEL>(h))));
+        DISPATCH(h->g.My, LAUNCH((launch_k2<LL, spns::MODE_VEL>(h))));
+        DISPATCH(h->g.Mz, LAUNCH((launch_k3<LL, spns::MODE_VEL>(h, phys))));
+        return SPNS_OK;
+    }
+
+    // E(K), Om(K) of the state into h->bins.
+    static int shell_sums(spns_handle *h) {
+        const int nb = h->last_rad_max + 1;
+        CK(cudaMemsetAsync(h->bins, 0, sizeof(double) * 2 * nb, h->st));
+        const long long n = h->g.S0;
+        const int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 8);
+        spns::k_shell_sums<T><<<blocks, 256, sizeof(double) * 2 * nb, h->st>>>(h->g, U(h, 0), U(h, 1), U(h, 2), Ulo(h, 0), Ulo(h, 1),
+                                                                              Ulo(h, 2), h->last_rad_max, h->bins, h->bins + nb);
+        CKL();
+        return SPNS_OK;
+    }
+
+    static int forcing_scale(spns_handle *h, int last_eff, int nullify) {
+        const long long n = h->g.S0;
+        const int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 16);
+        spns::k_forcing_scale<T><<<blocks, 256, 0, h->st>>>(h->g, U(h, 0), U(h, 1), U(h, 2), Ulo(h, 0), Ulo(h, 1), Ulo(h, 2), h->FT,
+                                                           last_eff, nullify);
+        CKL();
+        return SPNS_OK;
+    }
+
+    static int conj_correction(spns_handle *h) {
+        spns::k_conj_correction<T><<<64, 256, 0, h->st>>>(h->g, U(h, 0), U(h, 1), U(h, 2), Ulo(h, 0), Ulo(h, 1), Ulo(h, 2));
+        CKL();
+        return SPNS_OK;
+    }
+
+    // Exact aliasing correction of the rotational form on the +-N/2 planes
+    // (edge_kernels.cuh), added to the compact nonlinear term G held in B2.
+    static int edge_correction(spns_handle *h) {
+        const spns::Geo &g = h->g;
+        for (int axis = 0; axis < 3; axis++) {
+            if (!h->edge_axis[axis]) continue;
+            spns::EdgePlanes ep;
+            ep.axis = axis;
+            ep.nplanes = axis == 2 ? 1 : 2;
+            ep.R = axis == 0 ? g.My : g.Mx;
+            ep.C = axis == 2 ? g.My : g.Mz;
+            const long long n = (long long)ep.R * ep.C;
+            C *V = (C *)h->edge, *Phi = V + 3 * 2 * n;
+            const long long nb = n * 3 * ep.nplanes;
+            const int blocks = (int)std::min<long long>((nb + 255) / 256, 148 * 16);
+            spns::k_edge_build<T><<<blocks, 256, 0, h->st>>>(g, U(h), ep, V);
+            CKL();
+            DISPATCH(ep.C, LAUNCH((launch_lines<LL, true>(h, V, (long long)ep.R * 3 * ep.nplanes))));
+            DISPATCH(ep.R, LAUNCH((launch_cols<LL, true>(h, V, ep.C, 3 * ep.nplanes))));
+            spns::k_edge_square<T><<<blocks, 256, 0, h->st>>>(V, n, ep.nplanes, Phi);
+            CKL();
+            DISPATCH(ep.C, LAUNCH((launch_lines<LL, false>(h, Phi, (long long)ep.R * ep.nplanes))));
+            DISPATCH(ep.R, LAUNCH((launch_cols<LL, false>(h, Phi, ep.C, ep.nplanes))));
+            spns::k_edge_apply<T><<<blocks, 256, 0, h->st>>>(g, (C *)h->B2, ep, Phi);
+            CKL();
+        }
+        return SPNS_OK;
+    }
+
+    // Records an event before the next kernel of a profiled step.
+    static void prof_mark(spns_handle *h, int slot, const char *name) {
+        if (h->prof_steps >= h->prof_cap_steps) return;
+        if (slot >= 16) return;
+        if (h->prof_steps == 0 && (int)h->prof_names.size() <= slot) h->prof_names.push_back(name ? name : "");
+        cudaEventRecord(h->prof_ev[(size_t)h->prof_steps * 16 + slot], h->st);
+    }
+
+    // One New_Fractional_Step_Method (src/HIT_LES.cpp:9-25).
+    static int step_once(spns_handle *h) {
+        int nk = 0;
+        int slot = 0;
+        const bool prof = h->prof_steps < h->prof_cap_steps;
+#define MARK(name) do { if (prof) prof_mark(h, slot++, name); } while (0)
+        if (h->a.eps_forcing > 0.0) {
+            MARK("shell_sums");
+            int r = shell_sums(h);
+            if (r) return r;
+            MARK("eps_alpha");
+            spns::k_eps_alpha<<<1, 1, 0, h->st>>>(h->bins, h->a.eps_kmin, h->a.eps_kmax, h->a.eps_forcing, h->ds);
+            CKL();
+            nk += 2;
+        }
+        const int mode = h->a.isLES ? spns::MODE_LES : h->a.nonlinear_form == 2 ? spns::MODE_ADV : spns::MODE_ROT;
+#define STEP_PASSES(MD)                                                                       \
+        MARK("k1_inv_x");                                                                     \
+        DISPATCH(h->g.Mx, LAUNCH((launch_k1<LL, MD>(h))));                                    \
+        MARK("k2_inv_y");                                                                     \
+        DISPATCH(h->g.My, LAUNCH((launch_k2<LL, MD>(h))));                                    \
+        MARK("reset_max");                                                                    \
+        spns::k_reset_max<<<1, 1, 0, h->st>>>(h->ds);                                         \
+        CKL();                                                                                \
+        MARK("k3_z");                                                                         \
+        DISPATCH(h->g.Mz, LAUNCH((launch_k3<LL, MD>(h, nullptr))));                           \
+        MARK("k4_fwd_y");                                                                     \
+        DISPATCH(h->g.My, LAUNCH((launch_k4<LL, MD>(h))));                                    \
+        MARK("k5_fwd_x");                                                                     \
+        DISPATCH(h->g.Mx, LAUNCH((launch_k5<LL, MD>(h))));                                    \
+        if (MD == spns::MODE_ROT && h->edge) {                                                \
+            MARK("edge_correction");                                                          \
+            int r_ = edge_correction(h);                                                      \
+            if (r_) return r_;                                                                \
+        }                                                                                     \
+        MARK("k6_sweep");                                                                     \
+        LAUNCH(launch_k6(h));
+        if (mode == spns::MODE_LES) { STEP_PASSES(spns::MODE_LES) }
+        else if (mode == spns::MODE_ROT) { STEP_PASSES(spns::MODE_ROT) }
+        else { STEP_PASSES(spns::MODE_ADV) }
+#undef STEP_PASSES
+        MARK("finish_step");
+        spns::k_finish_step<<<1, 1, 0, h->st>>>(h->c, h->ds);
+        CKL();
+        MARK(nullptr);
+        if (prof) { if (h->prof_steps == 0) h->prof_nk = slot - 1; h->prof_steps++; }
+        if (mode == spns::MODE_ROT && h->edge)
+            for (int axis = 0; axis < 3; axis++) nk += h->edge_axis[axis] ? 7 : 0;   // build, 2+2 line FFTs, square, apply
+        h->kernels_per_step = nk + 8;
+        return SPNS_OK;
+#undef MARK
+    }
+
+    static constexpr PrecOps ops() {
+        return PrecOps{&step_once, &run_velocity, &shell_sums, &forcing_scale, &conj_correction};
+    }
+};

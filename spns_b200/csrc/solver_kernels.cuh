@@ -595,10 +595,17 @@ __global__ void __launch_bounds__(P *(L / E), 2) k5_fwd_x(Geo g, const cx<T> *__
 //   src/HIT_LES.cpp:346-359  projection  u -= k (k.u)/k^2
 // G holds the un-normalised nonlinear term (x1/M^3 here).  Kappa scheme: the
 // new state is written over the u^{n-1} buffer Un1 and the caller swaps U/Un1.
+// Single precision (T = float) is the compensated form: the states u^n, u^{n-1}
+// and u^{n+1} are pairs hi + lo of floats (about 48 significant bits) that this
+// sweep combines and splits in double, so the small increments dt*R are not
+// rounded away; G and R are plain floats.  In double precision the lo pointers
+// are unused (null).
 // ===========================================================================
 template <typename T, bool SELF>
-__global__ void __launch_bounds__(256) k6_sweep(Geo g, const cx<T> *__restrict__ G, const cx<T> *U, cx<T> *R, cx<T> *Uout,
-                                                const cx<T> *Un1, StepConsts c, const DevScalars *__restrict__ ds) {
+__global__ void __launch_bounds__(256) k6_sweep(Geo g, const cx<T> *__restrict__ G, const cx<T> *U, const cx<T> *Ulo, cx<T> *R,
+                                                cx<T> *Uout, cx<T> *Uoutlo, const cx<T> *Un1, const cx<T> *Un1lo, StepConsts c,
+                                                const DevScalars *__restrict__ ds) {
+    constexpr bool HILO = sizeof(T) == 4;
     const int iy = blockIdx.y;
     const int n = g.Kx * g.Kz;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -607,14 +614,22 @@ __global__ void __launch_bounds__(256) k6_sweep(Geo g, const cx<T> *__restrict__
     const long long idx = (long long)iy * n + t;
     const long long S0 = g.S0;
     // loads first
-    cx<T> gg[3], uu[3], r0[3], up[3];
+    cx<T> gg[3], uu[3], r0[3], up[3], ul[3], upl[3];
 #pragma unroll
     for (int i = 0; i < 3; i++) { gg[i] = G[i * S0 + idx]; uu[i] = U[i * S0 + idx]; r0[i] = R[i * S0 + idx]; }
+    if constexpr (HILO) {
+#pragma unroll
+        for (int i = 0; i < 3; i++) ul[i] = Ulo[i * S0 + idx];
+    }
     const double nu = ds->nu, dt = ds->dt, kap = ds->kappa, alpha = ds->alpha;
     const bool first = ds->iter == 0;
     if (SELF) {
 #pragma unroll
         for (int i = 0; i < 3; i++) up[i] = first ? uu[i] : Un1[i * S0 + idx];
+        if constexpr (HILO) {
+#pragma unroll
+            for (int i = 0; i < 3; i++) upl[i] = first ? ul[i] : Un1lo[i * S0 + idx];
+        }
     }
     const int m1 = ix <= g.hx ? ix : ix - g.Kx, m2 = iy <= g.hy ? iy : iy - g.Ky;
     const long long k1 = (long long)g.sx * m1, k2 = (long long)g.sy * m2, k3 = (long long)g.sz * kz;
@@ -625,6 +640,7 @@ __global__ void __launch_bounds__(256) k6_sweep(Geo g, const cx<T> *__restrict__
 #pragma unroll
     for (int i = 0; i < 3; i++) {
         ur[i] = uu[i].x; ui[i] = uu[i].y;
+        if constexpr (HILO) { ur[i] += (double)ul[i].x; ui[i] += (double)ul[i].y; }
         const double gr = mean ? 0.0 : (double)gg[i].x * c.inv_norm;
         const double gi = mean ? 0.0 : (double)gg[i].y * c.inv_norm;
         rr[i] = -gr - ct * ur[i];
@@ -650,8 +666,10 @@ __global__ void __launch_bounds__(256) k6_sweep(Geo g, const cx<T> *__restrict__
 #pragma unroll
     for (int i = 0; i < 3; i++) {
         if (SELF) {
-            sr[i] = k05 * (2.0 * kap * ur[i] + dt * ((1.0 + kap) * rr[i] - kap * (double)r0[i].x) - (kap - 0.5) * (double)up[i].x);
-            si[i] = k05 * (2.0 * kap * ui[i] + dt * ((1.0 + kap) * ri[i] - kap * (double)r0[i].y) - (kap - 0.5) * (double)up[i].y);
+            double pr = (double)up[i].x, pi = (double)up[i].y;
+            if constexpr (HILO) { pr += (double)upl[i].x; pi += (double)upl[i].y; }
+            sr[i] = k05 * (2.0 * kap * ur[i] + dt * ((1.0 + kap) * rr[i] - kap * (double)r0[i].x) - (kap - 0.5) * pr);
+            si[i] = k05 * (2.0 * kap * ui[i] + dt * ((1.0 + kap) * ri[i] - kap * (double)r0[i].y) - (kap - 0.5) * pi);
         } else {
             sr[i] = ur[i] + dt * (1.5 * rr[i] - 0.5 * (double)r0[i].x);
             si[i] = ui[i] + dt * (1.5 * ri[i] - 0.5 * (double)r0[i].y);
@@ -668,7 +686,9 @@ __global__ void __launch_bounds__(256) k6_sweep(Geo g, const cx<T> *__restrict__
 #pragma unroll
     for (int i = 0; i < 3; i++) {
         R[i * S0 + idx] = mk<T>(T(rr[i]), T(ri[i]));
-        Uout[i * S0 + idx] = mk<T>(T(sr[i]), T(si[i]));
+        const T hr = T(sr[i]), hi = T(si[i]);
+        Uout[i * S0 + idx] = mk<T>(hr, hi);
+        if constexpr (HILO) Uoutlo[i * S0 + idx] = mk<T>(T(sr[i] - (double)hr), T(si[i] - (double)hi));
     }
 }
 
@@ -744,8 +764,17 @@ static __global__ void k_reset_max(DevScalars *ds) {
 // Shell sums of the spectral state (src/HIT_LES.cpp:1137-1214 with the
 // KineticEnergy and Enstrophy integrands of :991-1003).  Modes with kz>0 carry
 // their conjugate (weight 2).  Ek[K], Om[K] for K=round(|k|) <= Kmax.
+// State value hi (+ lo when the compensated single-precision form passes one) in double.
+template <typename T> __device__ __forceinline__ cx<double> load_state(const cx<T> *hi, const cx<T> *lo, long long i) {
+    const cx<T> a = hi[i];
+    cx<double> r = mk<double>((double)a.x, (double)a.y);
+    if (lo) { const cx<T> b = lo[i]; r.x += (double)b.x; r.y += (double)b.y; }
+    return r;
+}
+
 template <typename T>
 __global__ void k_shell_sums(Geo g, const cx<T> *__restrict__ u, const cx<T> *__restrict__ v, const cx<T> *__restrict__ w,
+                             const cx<T> *__restrict__ ulo, const cx<T> *__restrict__ vlo, const cx<T> *__restrict__ wlo,
                              int Kmax, double *__restrict__ Ek, double *__restrict__ Om) {
     extern __shared__ double hist[];
     double *hE = hist, *hO = hist + (Kmax + 1);
@@ -762,9 +791,8 @@ __global__ void k_shell_sums(Geo g, const cx<T> *__restrict__ u, const cx<T> *__
         const double rad2 = (double)(k1 * k1 + k2 * k2 + k3 * k3);
         const int K = (int)round(sqrt(rad2));
         if (K > Kmax) continue;
-        const cx<T> a = u[idx], b = v[idx], cc = w[idx];
-        double e = 0.5 * ((double)a.x * a.x + (double)a.y * a.y + (double)b.x * b.x + (double)b.y * b.y + (double)cc.x * cc.x +
-                          (double)cc.y * cc.y);
+        const cx<double> a = load_state(u, ulo, idx), b = load_state(v, vlo, idx), cc = load_state(w, wlo, idx);
+        double e = 0.5 * (a.x * a.x + a.y * a.y + b.x * b.x + b.y * b.y + cc.x * cc.x + cc.y * cc.y);
         if (kz != 0) e *= 2.0;
         atomicAdd(&hE[K], e);
         atomicAdd(&hO[K], 2.0 * rad2 * e);
@@ -802,8 +830,11 @@ static __global__ void k_forcing_factors(const double *Ek, const double *Forced,
 }
 
 // src/HIT_LES.cpp:421-438: scale shells K<=last_eff, optionally zero the rest.
+// With lo parts (compensated single precision) the product is formed in double
+// and split again into hi + lo.
 template <typename T>
-__global__ void k_forcing_scale(Geo g, cx<T> *u, cx<T> *v, cx<T> *w, const double *FT, int last_eff, int nullify) {
+__global__ void k_forcing_scale(Geo g, cx<T> *u, cx<T> *v, cx<T> *w, cx<T> *ulo, cx<T> *vlo, cx<T> *wlo, const double *FT,
+                                int last_eff, int nullify) {
     const long long n = g.S0;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long long)gridDim.x * blockDim.x) {
         const int kz = (int)(idx % g.Kz);
@@ -814,10 +845,22 @@ __global__ void k_forcing_scale(Geo g, cx<T> *u, cx<T> *v, cx<T> *w, const doubl
         const long long k3 = (long long)g.sz * kz;
         const int K = (int)round(sqrt((double)(k1 * k1 + k2 * k2 + k3 * k3)));
         if (K <= last_eff) {
-            const T f = T(FT[K]);
-            u[idx] = f * u[idx]; v[idx] = f * v[idx]; w[idx] = f * w[idx];
+            if (ulo) {
+                cx<T> *hs[3] = {u, v, w}, *ls[3] = {ulo, vlo, wlo};
+                for (int i = 0; i < 3; i++) {
+                    const cx<double> x = load_state<T>(hs[i], ls[i], idx);
+                    const double xr = FT[K] * x.x, xi = FT[K] * x.y;
+                    const T hr = T(xr), hi = T(xi);
+                    hs[i][idx] = mk<T>(hr, hi);
+                    ls[i][idx] = mk<T>(T(xr - (double)hr), T(xi - (double)hi));
+                }
+            } else {
+                const T f = T(FT[K]);
+                u[idx] = f * u[idx]; v[idx] = f * v[idx]; w[idx] = f * w[idx];
+            }
         } else if (nullify) {
             u[idx] = zero<T>(); v[idx] = zero<T>(); w[idx] = zero<T>();
+            if (ulo) { ulo[idx] = zero<T>(); vlo[idx] = zero<T>(); wlo[idx] = zero<T>(); }
         }
     }
 }
@@ -825,7 +868,7 @@ __global__ void k_forcing_scale(Geo g, cx<T> *u, cx<T> *v, cx<T> *w, const doubl
 // src/HIT_LES.cpp:446-476 on the kz=0 plane: u(k1<0 or k1=0,k2<0) = conj(u(-k)).
 // The written and the read halves are disjoint, so no staging copy is needed.
 template <typename T>
-__global__ void k_conj_correction(Geo g, cx<T> *u, cx<T> *v, cx<T> *w) {
+__global__ void k_conj_correction(Geo g, cx<T> *u, cx<T> *v, cx<T> *w, cx<T> *ulo, cx<T> *vlo, cx<T> *wlo) {
     const int n = g.Kx * g.Ky;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
         const int ix = t % g.Kx, iy = t / g.Kx;
@@ -834,6 +877,7 @@ __global__ void k_conj_correction(Geo g, cx<T> *u, cx<T> *v, cx<T> *w) {
             const int jx = -m1, jy = -m2 >= 0 ? -m2 : -m2 + g.Ky;
             const long long dst = ((long long)iy * g.Kx + ix) * g.Kz, src = ((long long)jy * g.Kx + jx) * g.Kz;
             u[dst] = conj(u[src]); v[dst] = conj(v[src]); w[dst] = conj(w[src]);
+            if (ulo) { ulo[dst] = conj(ulo[src]); vlo[dst] = conj(vlo[src]); wlo[dst] = conj(wlo[src]); }
         }
     }
 }

@@ -1,111 +1,24 @@
-// spns.cu -- libspns: handle management, launch dispatch and the C ABI (include/spns.h).
+// spns.cu -- libspns: handle management, initial fields and the C ABI
+// (include/spns.h).  The passes of a step live in passes.cuh, instantiated per
+// precision in spns_f64.cu and spns_f32.cu.
 //
 // Every entry point forwards one member of the reference class HIT
 // (src/HIT_LES.h of adalbal/SpNS); see include/spns.h for the mapping.
-#include "spns.h"
-#include "solver_kernels.cuh"
-#include "edge_kernels.cuh"
+#include "handle.h"
 
-#include <cuda_runtime.h>
-
-#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
-#include <map>
-#include <string>
-#include <vector>
 
 using namespace spns;
-
-// ---------------------------------------------------------------------------
-// Compiled FFT lengths and launch shapes
-// ---------------------------------------------------------------------------
-#define SPNS_FOR_EACH_LENGTH(X) X(48) X(72) X(96) X(144) X(192) X(288) X(384) X(768) X(1536)
-
-static bool length_supported(int L) {
-#define SPNS_CASE(n) if (L == n) return true;
-    SPNS_FOR_EACH_LENGTH(SPNS_CASE)
-#undef SPNS_CASE
-    return false;
-}
-
-// Tile shapes per pass (complex values per thread E, threads per block),
-// chosen by timing the N=512 step on B200.
-template <typename T, int L, int E_, int THR> struct ShapeT {
-    static constexpr int E = E_;             // complex values per thread
-    static constexpr int Q = L / E;          // threads per pencil
-    static constexpr int P0 = THR / Q;
-    static constexpr int P = P0 >= 32 ? 32 : P0 >= 16 ? 16 : P0 >= 8 ? 8 : 4; // pencils per block
-    static constexpr int THREADS = P * Q;
-    static constexpr size_t SMEM_ROW = (size_t)L * P * sizeof(cx<T>);
-    static constexpr size_t SMEM_PEN = (size_t)SmPencil<T, L>::PITCH * P * sizeof(cx<T>);
-};
-template <typename T, int L> using ShapeK1 = ShapeT<T, L, 12, 256>;   // inverse x
-template <typename T, int L> using ShapeK2 = ShapeT<T, L, 24, 256>;   // inverse y (and forward y)
-template <typename T, int L> using ShapeK5 = ShapeT<T, L, 24, 128>;   // forward x
-template <typename T, int L> using Shape = ShapeT<T, L, 24, 128>;     // edge planes, test lines
-#ifndef SPNS_Z_THREADS
-#define SPNS_Z_THREADS 128    // threads per block in the z pass (2 blocks per SM)
-#endif
-#ifndef SPNS_Z_E
-#define SPNS_Z_E 12           // complex values per thread in the z pass (3 pairs in registers)
-#endif
-
-// z pass: pencils per block limited by the shared memory of the exchange
-// buffer plus the physical fields kept per pencil.
-template <typename T, int L, int MODE> struct Shape3 {
-    static constexpr int E = SPNS_Z_E;       // the z pass keeps several fields in registers
-    static constexpr int Q = L / E;
-    static constexpr int ZT = SPNS_Z_THREADS / Q;
-    static constexpr int P0 = ZT >= 32 ? 32 : ZT >= 16 ? 16 : ZT >= 8 ? 8 : ZT >= 4 ? 4 : ZT >= 2 ? 2 : 1;
-    static constexpr size_t PER_PEN = (size_t)SmPencil<T, L>::PITCH * sizeof(cx<T>) + (size_t)K3Phys<MODE>::N * L * sizeof(T);
-    static constexpr int PMAX = (int)((200 * 1024) / PER_PEN);
-    static constexpr int P = P0 <= PMAX ? P0 : PMAX >= 16 ? 16 : PMAX >= 8 ? 8 : PMAX >= 4 ? 4 : PMAX >= 2 ? 2 : 1;
-    static constexpr int THREADS = P * Q;
-    static constexpr size_t SMEM = PER_PEN * P;
-};
-
-// ---------------------------------------------------------------------------
-// Handle
-// ---------------------------------------------------------------------------
-struct spns_handle {
-    spns_hit_args a;
-    Geo g;
-    StepConsts c;
-    int last_rad = 0, last_rad_max = 0;
-    double delta = 0, Ek_init = 0, Ek_init_file = 0, Enstrophy_init_file = 0;
-    cudaStream_t st = nullptr;
-    DevScalars *ds = nullptr;
-    double2 *U = nullptr, *R = nullptr, *Up = nullptr; // 3 fields each (S0)
-    double2 *B1 = nullptr, *B2 = nullptr;            // S1 and S2 work buffers
-    int nB1 = 0, nB2 = 0;
-    double *bins = nullptr;                          // Ek[0..Kmax], Om[0..Kmax]
-    double *FT = nullptr, *forced = nullptr;
-    int forced_cap = 0;
-    double *phys = nullptr;
-    double2 *edge = nullptr;                         // edge-correction planes (rotational form)
-    bool edge_axis[3] = {false, false, false};       // axes whose +-N/2 planes alias (M = 3h)
-    std::map<int, double2 *> tw;                     // twiddle tables per length
-    std::string err;
-    int kernels_per_step = 0;
-    // CUDA graphs of one step, per parity of the state-buffer swap (kappa scheme)
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    double2 *U0 = nullptr;                           // state buffer of parity 0
-    bool use_graphs = true;
-    // optional per-kernel event profile of the next steps (spns_profile_*)
-    std::vector<cudaEvent_t> prof_ev;
-    std::vector<std::string> prof_names;
-    int prof_cap_steps = 0, prof_steps = 0, prof_nk = 0;
-};
 
 static thread_local std::string g_create_error;
 
 // Error text for calls that have no handle (reported by spns_last_error(NULL)).
 __attribute__((visibility("hidden"))) void spns_set_handleless_error(const char *msg) { g_create_error = msg; }
 
-static int fail(spns_handle *h, int code, const char *fmt, ...) {
+int spns_fail(spns_handle *h, int code, const char *fmt, ...) {
     char buf[1024];
     va_list ap;
     va_start(ap, fmt);
@@ -115,267 +28,52 @@ static int fail(spns_handle *h, int code, const char *fmt, ...) {
     return code;
 }
 
-#define CK(call)                                                                                   \
-    do {                                                                                           \
-        cudaError_t e_ = (call);                                                                   \
-        if (e_ != cudaSuccess)                                                                     \
-            return fail(h, e_ == cudaErrorMemoryAllocation ? SPNS_ERR_OUT_OF_MEMORY : SPNS_ERR_CUDA, \
-                        "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
-    } while (0)
-
-#define CKL()                                                                                      \
-    do {                                                                                           \
-        cudaError_t e_ = cudaGetLastError();                                                       \
-        if (e_ != cudaSuccess)                                                                     \
-            return fail(h, SPNS_ERR_CUDA, "kernel launch failed: %s (%s:%d)", cudaGetErrorString(e_), \
-                        __FILE__, __LINE__);                                                       \
-    } while (0)
-
 static int actual_n(int n, int L) { return (n % 2 == 0) ? n / L : (n - 1) / L + 1; }
 
-static double2 *make_twiddles(int L) {
-    std::vector<double2> t(L);
-    for (int m = 0; m < L; m++) {
-        long double ang = 2.0L * 3.14159265358979323846264338327950288L * (long double)m / (long double)L;
-        t[m] = make_double2((double)cosl(ang), (double)(-sinl(ang)));
-    }
-    double2 *d = nullptr;
-    if (cudaMalloc(&d, sizeof(double2) * L) != cudaSuccess) return nullptr;
-    if (cudaMemcpy(d, t.data(), sizeof(double2) * L, cudaMemcpyHostToDevice) != cudaSuccess) { cudaFree(d); return nullptr; }
-    return d;
-}
-
-template <class K> static cudaError_t set_smem(K kern, size_t bytes) {
-    if (bytes <= 48 * 1024) return cudaSuccess;
-    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-}
-
 // ---------------------------------------------------------------------------
-// Typed launchers (FP64 plain form)
+// State transfer between a host array of complex doubles and the device state
+// (double, or the float hi + lo pair of the compensated form).
 // ---------------------------------------------------------------------------
-using T64 = double;
-
-template <int L, int MODE> static cudaError_t launch_k1(spns_handle *h) {
-    using S = ShapeK1<T64, L>;
-    auto kern = k1_inv_x<T64, L, S::E, S::P, MODE>;
-    cudaError_t e = set_smem(kern, S::SMEM_ROW);
-    if (e != cudaSuccess) return e;
-    dim3 grid((h->g.Kz + S::P - 1) / S::P, h->g.Ky);
-    kern<<<grid, S::THREADS, S::SMEM_ROW, h->st>>>(h->g, (const cx<T64> *)h->U, (const cx<T64> *)(h->U + h->g.S0),
-                                                  (const cx<T64> *)(h->U + 2 * h->g.S0), (cx<T64> *)h->B1,
-                                                  (const cx<T64> *)h->tw[L]);
-    return cudaGetLastError();
-}
-template <int L, int MODE> static cudaError_t launch_k2(spns_handle *h) {
-    using S = ShapeK2<T64, L>;
-    auto kern = k2_inv_y<T64, L, S::E, S::P, MODE>;
-    cudaError_t e = set_smem(kern, S::SMEM_ROW);
-    if (e != cudaSuccess) return e;
-    dim3 grid((h->g.Kz + S::P - 1) / S::P, h->g.Mx);
-    kern<<<grid, S::THREADS, S::SMEM_ROW, h->st>>>(h->g, (const cx<T64> *)h->B1, (cx<T64> *)h->B2, (const cx<T64> *)h->tw[L]);
-    return cudaGetLastError();
-}
-template <int L, int MODE> static cudaError_t launch_k3(spns_handle *h, double *phys) {
-    using S3 = Shape3<T64, L, MODE>;
-    auto kern = k3_z<T64, L, S3::E, S3::P, MODE>;
-    cudaError_t e = set_smem(kern, S3::SMEM);
-    if (e != cudaSuccess) return e;
-    const long long npen = (long long)h->g.Mx * h->g.My;
-    dim3 grid((unsigned)((npen + S3::P - 1) / S3::P));
-    kern<<<grid, S3::THREADS, S3::SMEM, h->st>>>(h->g, (cx<T64> *)h->B2, h->c, h->ds, phys, (const cx<T64> *)h->tw[L]);
-    return cudaGetLastError();
-}
-template <int L, int MODE> static cudaError_t launch_k4(spns_handle *h) {
-    using S = ShapeK2<T64, L>;
-    auto kern = k4_fwd_y<T64, L, S::E, S::P, MODE>;
-    cudaError_t e = set_smem(kern, S::SMEM_ROW);
-    if (e != cudaSuccess) return e;
-    dim3 grid((h->g.Kz + S::P - 1) / S::P, h->g.Mx);
-    kern<<<grid, S::THREADS, S::SMEM_ROW, h->st>>>(h->g, (const cx<T64> *)h->B2, (cx<T64> *)h->B1, (const cx<T64> *)h->tw[L]);
-    return cudaGetLastError();
-}
-template <int L, int MODE> static cudaError_t launch_k5(spns_handle *h) {
-    using S = ShapeK5<T64, L>;
-    auto kern = k5_fwd_x<T64, L, S::E, S::P, MODE>;
-    cudaError_t e = set_smem(kern, S::SMEM_ROW);
-    if (e != cudaSuccess) return e;
-    dim3 grid((h->g.Kz + S::P - 1) / S::P, h->g.Ky);
-    kern<<<grid, S::THREADS, S::SMEM_ROW, h->st>>>(h->g, (const cx<T64> *)h->B1, (cx<T64> *)h->B2, (const cx<T64> *)h->tw[L]);
-    return cudaGetLastError();
-}
-// Spectral sweep; with the kappa scheme the new state goes into the u^{n-1}
-// buffer and the two state buffers are swapped after the launch.
-static cudaError_t launch_k6(spns_handle *h) {
-    const int n = h->g.Kx * h->g.Kz;
-    dim3 grid((n + 255) / 256, h->g.Ky);
-    if (h->a.isSelfAdaptive) {
-        k6_sweep<T64, true><<<grid, 256, 0, h->st>>>(h->g, (const cx<T64> *)h->B2, (const cx<T64> *)h->U, (cx<T64> *)h->R,
-                                                     (cx<T64> *)h->Up, (const cx<T64> *)h->Up, h->c, h->ds);
-        std::swap(h->U, h->Up);
-    } else {
-        k6_sweep<T64, false><<<grid, 256, 0, h->st>>>(h->g, (const cx<T64> *)h->B2, (const cx<T64> *)h->U, (cx<T64> *)h->R,
-                                                      (cx<T64> *)h->U, nullptr, h->c, h->ds);
+static int upload_state(spns_handle *h, const double2 *uvw) {
+    const size_t n = 3 * (size_t)h->g.S0;
+    if (h->prec == SPNS_FP64) {
+        CK(cudaMemcpyAsync(h->U, uvw, sizeof(double2) * n, cudaMemcpyHostToDevice, h->st));
+        CK(cudaStreamSynchronize(h->st));
+        return SPNS_OK;
     }
-    return cudaGetLastError();
-}
-
-// Batched 1-D FFTs for the 2-D edge planes.
-template <int L, bool INV> static cudaError_t launch_lines(spns_handle *h, double2 *data, long long batch) {
-    using S = Shape<T64, L>;
-    auto kern = k_lines<T64, L, S::E, S::P, INV>;
-    cudaError_t e = set_smem(kern, S::SMEM_PEN);
-    if (e != cudaSuccess) return e;
-    kern<<<(unsigned)((batch + S::P - 1) / S::P), S::THREADS, S::SMEM_PEN, h->st>>>((cx<T64> *)data, batch, (const cx<T64> *)h->tw[L]);
-    return cudaGetLastError();
-}
-template <int L, bool INV> static cudaError_t launch_cols(spns_handle *h, double2 *data, int ncols, int nbatch) {
-    using S = Shape<T64, L>;
-    auto kern = k_cols<T64, L, S::E, S::P, INV>;
-    cudaError_t e = set_smem(kern, S::SMEM_ROW);
-    if (e != cudaSuccess) return e;
-    dim3 grid((ncols + S::P - 1) / S::P, nbatch);
-    kern<<<grid, S::THREADS, S::SMEM_ROW, h->st>>>((cx<T64> *)data, ncols, (const cx<T64> *)h->tw[L]);
-    return cudaGetLastError();
-}
-
-#define DISPATCH(Lval, call)                                                                 \
-    switch (Lval) {                                                                          \
-    case 48: { constexpr int LL = 48; call; } break;                                         \
-    case 72: { constexpr int LL = 72; call; } break;                                         \
-    case 96: { constexpr int LL = 96; call; } break;                                         \
-    case 144: { constexpr int LL = 144; call; } break;                                       \
-    case 192: { constexpr int LL = 192; call; } break;                                       \
-    case 288: { constexpr int LL = 288; call; } break;                                       \
-    case 384: { constexpr int LL = 384; call; } break;                                       \
-    case 768: { constexpr int LL = 768; call; } break;                                       \
-    case 1536: { constexpr int LL = 1536; call; } break;                                     \
-    default: return fail(h, SPNS_ERR_UNSUPPORTED_SIZE, "FFT length %d is not compiled", Lval); \
+    std::vector<float2> hi(n), lo(n);
+    for (size_t i = 0; i < n; i++) {
+        const float hx = (float)uvw[i].x, hy = (float)uvw[i].y;
+        hi[i] = make_float2(hx, hy);
+        lo[i] = make_float2((float)(uvw[i].x - (double)hx), (float)(uvw[i].y - (double)hy));
     }
-
-#define LAUNCH(expr)                                                                              \
-    do {                                                                                          \
-        cudaError_t e_ = (expr);                                                                  \
-        if (e_ != cudaSuccess)                                                                    \
-            return fail(h, SPNS_ERR_CUDA, "launch failed: %s (%s:%d)", cudaGetErrorString(e_), __FILE__, __LINE__); \
-    } while (0)
-
-// Inverse transform of the velocity only (Recalculate_Velocity_Antitransform):
-// refreshes the CFL maxima and, if phys != NULL, writes u,v,w on the grid.
-static int run_velocity(spns_handle *h, double *phys) {
-    k_reset_max<<<1, 1, 0, h->st>>>(h->ds);
-    CKL();
-    DISPATCH(h->g.Mx, LAUNCH((launch_k1<LL, MODE_VEL>(h))));
-    DISPATCH(h->g.My, LAUNCH((launch_k2<LL, MODE_VEL>(h))));
-    DISPATCH(h->g.Mz, LAUNCH((launch_k3<LL, MODE_VEL>(h, phys))));
+    CK(cudaMemcpyAsync(h->U, hi.data(), sizeof(float2) * n, cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(h->Ulo, lo.data(), sizeof(float2) * n, cudaMemcpyHostToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));
     return SPNS_OK;
 }
 
-static int shell_sums(spns_handle *h, int bx, int by, int bz) {
-    (void)bx; (void)by; (void)bz;
-    const int nb = h->last_rad_max + 1;
-    CK(cudaMemsetAsync(h->bins, 0, sizeof(double) * 2 * nb, h->st));
-    const long long n = h->g.S0;
-    int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 8);
-    k_shell_sums<T64><<<blocks, 256, sizeof(double) * 2 * nb, h->st>>>(
-        h->g, (const cx<T64> *)h->U, (const cx<T64> *)(h->U + h->g.S0), (const cx<T64> *)(h->U + 2 * h->g.S0), h->last_rad_max,
-        h->bins, h->bins + nb);
-    CKL();
-    return SPNS_OK;
-}
-
-// Exact aliasing correction of the rotational form on the +-N/2 planes
-// (edge_kernels.cuh), added to the compact nonlinear term G held in B2.
-static int edge_correction(spns_handle *h) {
-    const Geo &g = h->g;
-    for (int axis = 0; axis < 3; axis++) {
-        if (!h->edge_axis[axis]) continue;
-        EdgePlanes ep;
-        ep.axis = axis;
-        ep.nplanes = axis == 2 ? 1 : 2;
-        ep.R = axis == 0 ? g.My : g.Mx;
-        ep.C = axis == 2 ? g.My : g.Mz;
-        const long long n = (long long)ep.R * ep.C;
-        double2 *V = h->edge, *Phi = h->edge + 3 * 2 * n;
-        const long long nb = n * 3 * ep.nplanes;
-        const int blocks = (int)std::min<long long>((nb + 255) / 256, 148 * 16);
-        k_edge_build<T64><<<blocks, 256, 0, h->st>>>(g, (const cx<T64> *)h->U, ep, (cx<T64> *)V);
-        CKL();
-        DISPATCH(ep.C, LAUNCH((launch_lines<LL, true>(h, V, (long long)ep.R * 3 * ep.nplanes))));
-        DISPATCH(ep.R, LAUNCH((launch_cols<LL, true>(h, V, ep.C, 3 * ep.nplanes))));
-        k_edge_square<T64><<<blocks, 256, 0, h->st>>>((const cx<T64> *)V, n, ep.nplanes, (cx<T64> *)Phi);
-        CKL();
-        DISPATCH(ep.C, LAUNCH((launch_lines<LL, false>(h, Phi, (long long)ep.R * ep.nplanes))));
-        DISPATCH(ep.R, LAUNCH((launch_cols<LL, false>(h, Phi, ep.C, ep.nplanes))));
-        k_edge_apply<T64><<<blocks, 256, 0, h->st>>>(g, (cx<T64> *)h->B2, ep, (const cx<T64> *)Phi);
-        CKL();
+static int download_state(spns_handle *h, double2 *uvw) {
+    const size_t n = 3 * (size_t)h->g.S0;
+    if (h->prec == SPNS_FP64) {
+        CK(cudaMemcpyAsync(uvw, h->U, sizeof(double2) * n, cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
+        return SPNS_OK;
     }
+    std::vector<float2> hi(n), lo(n);
+    CK(cudaMemcpyAsync(hi.data(), h->U, sizeof(float2) * n, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaMemcpyAsync(lo.data(), h->Ulo, sizeof(float2) * n, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    for (size_t i = 0; i < n; i++) uvw[i] = make_double2((double)hi[i].x + (double)lo[i].x, (double)hi[i].y + (double)lo[i].y);
     return SPNS_OK;
-}
-
-// Records an event before the next kernel of a profiled step.
-static void prof_mark(spns_handle *h, int slot, const char *name) {
-    if (h->prof_steps >= h->prof_cap_steps) return;
-    if (slot >= 16) return;
-    if (h->prof_steps == 0 && (int)h->prof_names.size() <= slot) h->prof_names.push_back(name ? name : "");
-    cudaEventRecord(h->prof_ev[(size_t)h->prof_steps * 16 + slot], h->st);
-}
-
-static int step_once(spns_handle *h) {
-    int nk = 0;
-    int slot = 0;
-    const bool prof = h->prof_steps < h->prof_cap_steps;
-#define MARK(name) do { if (prof) prof_mark(h, slot++, name); } while (0)
-    if (h->a.eps_forcing > 0.0) {
-        MARK("shell_sums");
-        int r = shell_sums(h, 0, 0, 0);
-        if (r) return r;
-        MARK("eps_alpha");
-        k_eps_alpha<<<1, 1, 0, h->st>>>(h->bins, h->a.eps_kmin, h->a.eps_kmax, h->a.eps_forcing, h->ds);
-        CKL();
-        nk += 2;
-    }
-    const int mode = h->a.isLES ? MODE_LES : h->a.nonlinear_form == 2 ? MODE_ADV : MODE_ROT;
-#define STEP_PASSES(MD)                                                                       \
-    MARK("k1_inv_x");                                                                         \
-    DISPATCH(h->g.Mx, LAUNCH((launch_k1<LL, MD>(h))));                                        \
-    MARK("k2_inv_y");                                                                         \
-    DISPATCH(h->g.My, LAUNCH((launch_k2<LL, MD>(h))));                                        \
-    MARK("reset_max");                                                                        \
-    k_reset_max<<<1, 1, 0, h->st>>>(h->ds);                                                   \
-    CKL();                                                                                    \
-    MARK("k3_z");                                                                             \
-    DISPATCH(h->g.Mz, LAUNCH((launch_k3<LL, MD>(h, nullptr))));                               \
-    MARK("k4_fwd_y");                                                                         \
-    DISPATCH(h->g.My, LAUNCH((launch_k4<LL, MD>(h))));                                        \
-    MARK("k5_fwd_x");                                                                         \
-    DISPATCH(h->g.Mx, LAUNCH((launch_k5<LL, MD>(h))));                                        \
-    if (MD == MODE_ROT && h->edge) {                                                          \
-        MARK("edge_correction");                                                              \
-        int r_ = edge_correction(h);                                                          \
-        if (r_) return r_;                                                                    \
-    }                                                                                         \
-    MARK("k6_sweep");                                                                         \
-    LAUNCH(launch_k6(h));
-    if (mode == MODE_LES) { STEP_PASSES(MODE_LES) }
-    else if (mode == MODE_ROT) { STEP_PASSES(MODE_ROT) }
-    else { STEP_PASSES(MODE_ADV) }
-#undef STEP_PASSES
-    MARK("finish_step");
-    k_finish_step<<<1, 1, 0, h->st>>>(h->c, h->ds);
-    CKL();
-    MARK(nullptr);
-    if (prof) { if (h->prof_steps == 0) h->prof_nk = slot - 1; h->prof_steps++; }
-    h->kernels_per_step = nk + 8;
-    return SPNS_OK;
-#undef MARK
 }
 
 static int check_flags(spns_handle *h) {
     DevScalars s;
     CK(cudaMemcpyAsync(&s, h->ds, sizeof(s), cudaMemcpyDeviceToHost, h->st));
     CK(cudaStreamSynchronize(h->st));
-    if (s.nonfinite) return fail(h, SPNS_ERR_NONFINITE, "non-finite velocity met in the CFL maximum (iter %lld)", s.iter);
-    if (s.domain_err) return fail(h, SPNS_ERR_DOMAIN, "Topt fail! (time-step angle outside [0, pi/2])");
+    if (s.nonfinite) return spns_fail(h, SPNS_ERR_NONFINITE, "non-finite velocity met in the CFL maximum (iter %lld)", s.iter);
+    if (s.domain_err) return spns_fail(h, SPNS_ERR_DOMAIN, "Topt fail! (time-step angle outside [0, pi/2])");
     return SPNS_OK;
 }
 
@@ -443,8 +141,9 @@ static int file_init(spns_handle *h, const double *file_uvw, std::vector<double2
     CK(cudaMalloc(&d_b, sizeof(double2) * nspec));
     int maxn = std::max(nx, std::max(ny, nz));
     CK(cudaMalloc(&d_k, sizeof(int) * maxn));
-    twx = make_twiddles(nx); twy = make_twiddles(ny); twz = make_twiddles(nz);
-    if (!twx || !twy || !twz) return fail(h, SPNS_ERR_OUT_OF_MEMORY, "twiddle allocation failed");
+    twx = (double2 *)spns_make_twiddles<double>(nx); twy = (double2 *)spns_make_twiddles<double>(ny);
+    twz = (double2 *)spns_make_twiddles<double>(nz);
+    if (!twx || !twy || !twz) return spns_fail(h, SPNS_ERR_OUT_OF_MEMORY, "twiddle allocation failed");
     std::vector<int> kk(maxn);
     for (int i = 0; i < maxn; i++) kk[i] = i;
     CK(cudaMemcpy(d_k, kk.data(), sizeof(int) * maxn, cudaMemcpyHostToDevice));
@@ -507,7 +206,7 @@ static int file_init(spns_handle *h, const double *file_uvw, std::vector<double2
 // Helpers for API calls
 // ---------------------------------------------------------------------------
 static int forcing_energy_cascade(spns_handle *h, const double *Forced, int last_input_rad, int nullify) {
-    int r = shell_sums(h, 0, 0, 0);
+    int r = spns_ops(h).shell_sums(h);
     if (r) return r;
     const int nb = h->last_rad_max + 1;
     k_totals<<<1, 1, 0, h->st>>>(h->bins, h->bins + nb, h->last_rad_max, h->ds, 0, 0.0);
@@ -524,14 +223,11 @@ static int forcing_energy_cascade(spns_handle *h, const double *Forced, int last
     CK(cudaMemcpyAsync(h->forced, Forced, sizeof(double) * (last_eff + 1), cudaMemcpyHostToDevice, h->st));
     k_forcing_factors<<<1, 256, 0, h->st>>>(h->bins, h->forced, last_eff, h->FT);
     CKL();
-    const long long n = h->g.S0;
-    int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 16);
-    k_forcing_scale<T64><<<blocks, 256, 0, h->st>>>(h->g, (cx<T64> *)h->U, (cx<T64> *)(h->U + n), (cx<T64> *)(h->U + 2 * n), h->FT,
-                                                    last_eff, nullify);
-    CKL();
+    r = spns_ops(h).forcing_scale(h, last_eff, nullify);
+    if (r) return r;
     if (h->a.isComplexConjugateCorrected) {
-        k_conj_correction<T64><<<64, 256, 0, h->st>>>(h->g, (cx<T64> *)h->U, (cx<T64> *)(h->U + n), (cx<T64> *)(h->U + 2 * n));
-        CKL();
+        r = spns_ops(h).conj_correction(h);
+        if (r) return r;
     }
     // The forced state must be visible before the caller frees Forced.
     CK(cudaStreamSynchronize(h->st));
@@ -539,7 +235,7 @@ static int forcing_energy_cascade(spns_handle *h, const double *Forced, int last
 }
 
 static int totals(spns_handle *h, int what, double relambda) {
-    int r = shell_sums(h, 0, 0, 0);
+    int r = spns_ops(h).shell_sums(h);
     if (r) return r;
     const int nb = h->last_rad_max + 1;
     k_totals<<<1, 1, 0, h->st>>>(h->bins, h->bins + nb, h->last_rad_max, h->ds, what, relambda);
@@ -555,7 +251,8 @@ static int read_scalars(spns_handle *h, DevScalars *s) {
 
 static void free_handle(spns_handle *h) {
     if (!h) return;
-    cudaFree(h->ds); cudaFree(h->U); cudaFree(h->R); cudaFree(h->Up); cudaFree(h->B1); cudaFree(h->B2);
+    cudaFree(h->ds); cudaFree(h->U); cudaFree(h->Ulo); cudaFree(h->R); cudaFree(h->Up); cudaFree(h->Uplo);
+    cudaFree(h->B1); cudaFree(h->B2);
     cudaFree(h->bins); cudaFree(h->FT); cudaFree(h->forced); cudaFree(h->phys); cudaFree(h->edge);
     for (auto &kv : h->tw) cudaFree(kv.second);
     for (auto ev : h->prof_ev) cudaEventDestroy(ev);
@@ -586,19 +283,22 @@ const char *spns_last_error(spns_handle *h) { return h ? h->err.c_str() : g_crea
 
 int spns_create(const spns_hit_args *args, const double *file_uvw, spns_handle **out) {
     spns_handle *h = nullptr;
-    if (!args || !out) return fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "null argument");
+    if (!args || !out) return spns_fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "null argument");
     *out = nullptr;
-    if (args->precision != SPNS_FP64) return fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "precision %d not available in this build", args->precision);
+    if (args->precision != SPNS_FP64 && args->precision != SPNS_FP32_HILO)
+        return spns_fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "unknown precision %d", args->precision);
     if (args->Lx_factor < 1 || args->Ly_factor < 1 || args->Lz_factor < 1 || args->Nx < 2 || args->Ny < 2 || args->Nz < 2)
-        return fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "invalid sizes or length factors");
-    if (args->isInitialFieldFromFile && !file_uvw) return fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "file initial field requested without data");
+        return spns_fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "invalid sizes or length factors");
+    if (args->isInitialFieldFromFile && !file_uvw) return spns_fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "file initial field requested without data");
     h = new spns_handle();
     h->a = *args;
+    h->prec = args->precision;
+    h->csz = h->prec == SPNS_FP64 ? sizeof(double2) : sizeof(float2);
     const spns_hit_args &a = h->a;
     int rc;
     {
         cudaError_t e = cudaSetDevice(a.device);
-        if (e != cudaSuccess) { fail(nullptr, SPNS_ERR_CUDA, "cudaSetDevice(%d): %s", a.device, cudaGetErrorString(e)); delete h; return SPNS_ERR_CUDA; }
+        if (e != cudaSuccess) { spns_fail(nullptr, SPNS_ERR_CUDA, "cudaSetDevice(%d): %s", a.device, cudaGetErrorString(e)); delete h; return SPNS_ERR_CUDA; }
     }
     // geometry (true grid of a non-cubic box, src/HIT_LES.h:31-36)
     Geo &g = h->g;
@@ -611,12 +311,12 @@ int spns_create(const spns_hit_args *args, const double *file_uvw, spns_handle *
     g.S0 = (long long)g.Ky * g.Kx * g.Kz;
     g.S1 = (long long)g.Ky * g.Mx * g.Kz;
     g.S2 = (long long)g.My * g.Mx * g.Kz;
-    if (!length_supported(g.Mx) || !length_supported(g.My) || !length_supported(g.Mz)) {
-        rc = fail(nullptr, SPNS_ERR_UNSUPPORTED_SIZE, "FFT grid %dx%dx%d outside the compiled lengths", g.Mx, g.My, g.Mz);
+    if (!spns_length_supported(g.Mx) || !spns_length_supported(g.My) || !spns_length_supported(g.Mz)) {
+        rc = spns_fail(nullptr, SPNS_ERR_UNSUPPORTED_SIZE, "FFT grid %dx%dx%d outside the compiled lengths", g.Mx, g.My, g.Mz);
         delete h; return rc;
     }
     if (2 * g.hx >= g.Mx || 2 * g.hy >= g.My || 2 * g.hz >= g.Mz) {
-        rc = fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "retained modes do not fit the FFT grid");
+        rc = spns_fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "retained modes do not fit the FFT grid");
         delete h; return rc;
     }
     h->last_rad = std::min((a.Nx - 1) / 2, std::min((a.Ny - 1) / 2, (a.Nz - 1) / 2));
@@ -647,7 +347,7 @@ int spns_create(const spns_hit_args *args, const double *file_uvw, spns_handle *
 
     // device memory
     auto cleanup = [&](int code) { free_handle(h); return code; };
-    if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) return cleanup(fail(nullptr, SPNS_ERR_CUDA, "stream creation failed"));
+    if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) return cleanup(spns_fail(nullptr, SPNS_ERR_CUDA, "stream creation failed"));
     const bool rot = !a.isLES && a.nonlinear_form != 2;
     h->nB1 = rot ? 5 : 6;
     h->nB2 = rot ? 6 : 9;
@@ -656,44 +356,46 @@ int spns_create(const spns_hit_args *args, const double *file_uvw, spns_handle *
     h->edge_axis[1] = g.hy > 0 && g.My <= 3 * g.hy;
     h->edge_axis[2] = g.hz > 0 && g.Mz <= 3 * g.hz;
     const bool need_edge = rot && a.nonlinear_form == 0 && (h->edge_axis[0] || h->edge_axis[1] || h->edge_axis[2]);
-    size_t s0 = sizeof(double2) * 3 * g.S0;
+    const size_t cs = h->csz;
+    const size_t s0 = cs * 3 * g.S0;
+    const bool hilo = h->prec == SPNS_FP32_HILO;
     bool okm = cudaMalloc(&h->ds, sizeof(DevScalars)) == cudaSuccess && cudaMalloc(&h->U, s0) == cudaSuccess &&
-               cudaMalloc(&h->R, s0) == cudaSuccess &&
+               (!hilo || cudaMalloc(&h->Ulo, s0) == cudaSuccess) && cudaMalloc(&h->R, s0) == cudaSuccess &&
                (!a.isSelfAdaptive || cudaMalloc(&h->Up, s0) == cudaSuccess) &&
-               cudaMalloc(&h->B1, sizeof(double2) * h->nB1 * g.S1) == cudaSuccess &&
-               cudaMalloc(&h->B2, sizeof(double2) * h->nB2 * g.S2) == cudaSuccess &&
+               (!a.isSelfAdaptive || !hilo || cudaMalloc(&h->Uplo, s0) == cudaSuccess) &&
+               cudaMalloc(&h->B1, cs * h->nB1 * g.S1) == cudaSuccess &&
+               cudaMalloc(&h->B2, cs * h->nB2 * g.S2) == cudaSuccess &&
                cudaMalloc(&h->bins, sizeof(double) * 2 * (h->last_rad_max + 1)) == cudaSuccess &&
-               (!need_edge || cudaMalloc(&h->edge, sizeof(double2) * 8 *
+               (!need_edge || cudaMalloc(&h->edge, cs * 8 *
                                          (size_t)std::max((long long)g.My * g.Mz, std::max((long long)g.Mx * g.Mz, (long long)g.Mx * g.My))) == cudaSuccess);
-    if (!okm) { cudaGetLastError(); return cleanup(fail(nullptr, SPNS_ERR_OUT_OF_MEMORY, "device allocation failed")); }
+    if (!okm) { cudaGetLastError(); return cleanup(spns_fail(nullptr, SPNS_ERR_OUT_OF_MEMORY, "device allocation failed")); }
     for (int L : {g.Mx, g.My, g.Mz})
         if (!h->tw.count(L)) {
-            double2 *t = make_twiddles(L);
-            if (!t) return cleanup(fail(nullptr, SPNS_ERR_OUT_OF_MEMORY, "twiddle allocation failed"));
+            void *t = hilo ? spns_make_twiddles<float>(L) : spns_make_twiddles<double>(L);
+            if (!t) return cleanup(spns_fail(nullptr, SPNS_ERR_OUT_OF_MEMORY, "twiddle allocation failed"));
             h->tw[L] = t;
         }
     cudaMemset(h->R, 0, s0);
     if (h->Up) cudaMemset(h->Up, 0, s0);
+    if (h->Uplo) cudaMemset(h->Uplo, 0, s0);
     DevScalars s0v;
     memset(&s0v, 0, sizeof(s0v));
     s0v.nu = a.nu;
     s0v.kappa = 0.5;
     if (cudaMemcpy(h->ds, &s0v, sizeof(s0v), cudaMemcpyHostToDevice) != cudaSuccess)
-        return cleanup(fail(nullptr, SPNS_ERR_CUDA, "scalar upload failed"));
+        return cleanup(spns_fail(nullptr, SPNS_ERR_CUDA, "scalar upload failed"));
 
     // initial field
     std::vector<double2> uvw;
     if (a.isInitialFieldFromFile) {
         rc = file_init(h, file_uvw, uvw);
+        if (!rc) rc = upload_state(h, uvw.data());
         if (rc) { g_create_error = h->err; return cleanup(rc); }
-        if (cudaMemcpy(h->U, uvw.data(), s0, cudaMemcpyHostToDevice) != cudaSuccess)
-            return cleanup(fail(nullptr, SPNS_ERR_CUDA, "state upload failed"));
     } else {
         k41_host(h, uvw);
-        if (cudaMemcpy(h->U, uvw.data(), s0, cudaMemcpyHostToDevice) != cudaSuccess)
-            return cleanup(fail(nullptr, SPNS_ERR_CUDA, "state upload failed"));
-        const long long n = g.S0;
-        k_conj_correction<T64><<<64, 256, 0, h->st>>>(g, (cx<T64> *)h->U, (cx<T64> *)(h->U + n), (cx<T64> *)(h->U + 2 * n));
+        rc = upload_state(h, uvw.data());
+        if (!rc) rc = spns_ops(h).conj_correction(h);
+        if (rc) { g_create_error = h->err; return cleanup(rc); }
         std::vector<double> K41((size_t)h->last_rad + 1, 0.0);
         for (int K = 1; K <= h->last_rad; K++) K41[K] = std::pow((double)K, -5.0 / 3.0);
         rc = forcing_energy_cascade(h, K41.data(), h->last_rad, 0);
@@ -704,7 +406,7 @@ int spns_create(const spns_hit_args *args, const double *file_uvw, spns_handle *
         const char *ng = getenv("SPNS_NO_GRAPHS");
         h->use_graphs = !(ng && ng[0] == '1');
     }
-    rc = run_velocity(h, nullptr);
+    rc = spns_ops(h).run_velocity(h, nullptr);
     if (rc) { g_create_error = h->err; return cleanup(rc); }
     if (!a.isReLambda) {
         k_recalc_dt<<<1, 1, 0, h->st>>>(h->c, h->ds);
@@ -734,20 +436,20 @@ int spns_destroy(spns_handle *h) {
 static int step_graph(spns_handle *h) {
     const int par = (h->U == h->U0) ? 0 : 1;
     if (!h->graph[par]) {
-        double2 *U = h->U, *Up = h->Up;
+        void *U = h->U, *Up = h->Up, *Ulo = h->Ulo, *Uplo = h->Uplo;
         cudaGraph_t gr = nullptr;
         CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
-        int r = step_once(h);
+        int r = spns_ops(h).step_once(h);
         cudaError_t e = cudaStreamEndCapture(h->st, &gr);
-        h->U = U; h->Up = Up;
+        h->U = U; h->Up = Up; h->Ulo = Ulo; h->Uplo = Uplo;
         if (r) { if (gr) cudaGraphDestroy(gr); return r; }
-        if (e != cudaSuccess) return fail(h, SPNS_ERR_CUDA, "step capture failed: %s", cudaGetErrorString(e));
+        if (e != cudaSuccess) return spns_fail(h, SPNS_ERR_CUDA, "step capture failed: %s", cudaGetErrorString(e));
         e = cudaGraphInstantiate(&h->graph[par], gr, 0);
         cudaGraphDestroy(gr);
-        if (e != cudaSuccess) return fail(h, SPNS_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(e));
+        if (e != cudaSuccess) return spns_fail(h, SPNS_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(e));
     }
     CK(cudaGraphLaunch(h->graph[par], h->st));
-    if (h->a.isSelfAdaptive) std::swap(h->U, h->Up);
+    if (h->a.isSelfAdaptive) { std::swap(h->U, h->Up); std::swap(h->Ulo, h->Uplo); }
     return SPNS_OK;
 }
 
@@ -756,7 +458,7 @@ int spns_step(spns_handle *h, int nsteps) {
     for (int i = 0; i < nsteps; i++) {
         const bool profiling = h->prof_steps < h->prof_cap_steps;
         const bool warm = h->kernels_per_step > 0;   // a first step has run uncaptured
-        int r = (h->use_graphs && warm && !profiling) ? step_graph(h) : step_once(h);
+        int r = (h->use_graphs && warm && !profiling) ? step_graph(h) : spns_ops(h).step_once(h);
         if (r) return r;
     }
     return check_flags(h);
@@ -822,15 +524,12 @@ int spns_recalculate_energy_cascade(spns_handle *h, double *Ek, double *ek_tot) 
 
 int spns_velocity_antitransform(spns_handle *h) {
     if (!h) return SPNS_ERR_INVALID_ARGUMENT;
-    return run_velocity(h, nullptr);
+    return spns_ops(h).run_velocity(h, nullptr);
 }
 
 int spns_complex_conjugate_correction(spns_handle *h) {
     if (!h) return SPNS_ERR_INVALID_ARGUMENT;
-    const long long n = h->g.S0;
-    k_conj_correction<T64><<<64, 256, 0, h->st>>>(h->g, (cx<T64> *)h->U, (cx<T64> *)(h->U + n), (cx<T64> *)(h->U + 2 * n));
-    CKL();
-    return SPNS_OK;
+    return spns_ops(h).conj_correction(h);
 }
 
 int spns_check_physfour_energy(spns_handle *h, double atol, int *ok, double *d1, double *d2) {
@@ -841,7 +540,7 @@ int spns_check_physfour_energy(spns_handle *h, double atol, int *ok, double *d1,
     r = read_scalars(h, &s);
     if (r) return r;
     const double EkFour = s.ek_tot;
-    r = run_velocity(h, nullptr);
+    r = spns_ops(h).run_velocity(h, nullptr);
     if (r) return r;
     r = read_scalars(h, &s);
     if (r) return r;
@@ -889,23 +588,19 @@ int spns_physical_dims(spns_handle *h, int *Mx, int *My, int *Mz) {
 
 int spns_get_spectral(spns_handle *h, double *uvw) {
     if (!h || !uvw) return SPNS_ERR_INVALID_ARGUMENT;
-    CK(cudaMemcpyAsync(uvw, h->U, sizeof(double2) * 3 * h->g.S0, cudaMemcpyDeviceToHost, h->st));
-    CK(cudaStreamSynchronize(h->st));
-    return SPNS_OK;
+    return download_state(h, (double2 *)uvw);
 }
 
 int spns_set_spectral(spns_handle *h, const double *uvw) {
     if (!h || !uvw) return SPNS_ERR_INVALID_ARGUMENT;
-    CK(cudaMemcpyAsync(h->U, uvw, sizeof(double2) * 3 * h->g.S0, cudaMemcpyHostToDevice, h->st));
-    CK(cudaStreamSynchronize(h->st));
-    return SPNS_OK;
+    return upload_state(h, (const double2 *)uvw);
 }
 
 int spns_get_physical(spns_handle *h, double *uvw) {
     if (!h || !uvw) return SPNS_ERR_INVALID_ARGUMENT;
     const long long n3 = (long long)h->g.Mx * h->g.My * h->g.Mz;
     if (!h->phys) CK(cudaMalloc(&h->phys, sizeof(double) * 3 * n3));
-    int r = run_velocity(h, h->phys);
+    int r = spns_ops(h).run_velocity(h, h->phys);
     if (r) return r;
     CK(cudaMemcpyAsync(uvw, h->phys, sizeof(double) * 3 * n3, cudaMemcpyDeviceToHost, h->st));
     CK(cudaStreamSynchronize(h->st));
@@ -914,9 +609,11 @@ int spns_get_physical(spns_handle *h, double *uvw) {
 
 int spns_device_state(spns_handle *h, void **u, void **v, void **w) {
     if (!h) return SPNS_ERR_INVALID_ARGUMENT;
-    if (u) *u = h->U;
-    if (v) *v = h->U + h->g.S0;
-    if (w) *w = h->U + 2 * h->g.S0;
+    char *b = (char *)h->U;
+    const size_t fs = h->csz * (size_t)h->g.S0;
+    if (u) *u = b;
+    if (v) *v = b + fs;
+    if (w) *w = b + 2 * fs;
     return SPNS_OK;
 }
 
@@ -1006,15 +703,15 @@ __global__ void k_fft1d_lines(double2 *data, int batch, int sign, const double2 
 
 extern "C" int spns_fft1d_batch_f64(void *data_dev, int n, int batch, int sign) {
     spns_handle *h = nullptr;
-    if (!data_dev || batch < 0 || (sign != 1 && sign != -1)) return fail(h, SPNS_ERR_INVALID_ARGUMENT, "invalid argument");
-    if (!length_supported(n)) return fail(h, SPNS_ERR_UNSUPPORTED_SIZE, "FFT length %d is not compiled", n);
+    if (!data_dev || batch < 0 || (sign != 1 && sign != -1)) return spns_fail(h, SPNS_ERR_INVALID_ARGUMENT, "invalid argument");
+    if (!spns_length_supported(n)) return spns_fail(h, SPNS_ERR_UNSUPPORTED_SIZE, "FFT length %d is not compiled", n);
     static std::map<std::pair<int, int>, double2 *> tws;
     int dev = 0;
     cudaGetDevice(&dev);
     auto key = std::make_pair(dev, n);
     if (!tws.count(key)) {
-        double2 *t = make_twiddles(n);
-        if (!t) return fail(h, SPNS_ERR_OUT_OF_MEMORY, "twiddle allocation failed");
+        double2 *t = (double2 *)spns_make_twiddles<double>(n);
+        if (!t) return spns_fail(h, SPNS_ERR_OUT_OF_MEMORY, "twiddle allocation failed");
         tws[key] = t;
     }
     const double2 *tw = tws[key];
@@ -1022,12 +719,12 @@ extern "C" int spns_fft1d_batch_f64(void *data_dev, int n, int batch, int sign) 
     if (n == LL) {                                                                                \
         using S = Shape<double, LL>;                                                              \
         auto kern = k_fft1d_lines<LL>;                                                            \
-        if (set_smem(kern, S::SMEM_PEN) != cudaSuccess) return fail(h, SPNS_ERR_CUDA, "smem attribute"); \
+        if (spns_set_smem(kern, S::SMEM_PEN) != cudaSuccess) return spns_fail(h, SPNS_ERR_CUDA, "smem attribute"); \
         if (batch > 0) kern<<<(batch + S::P - 1) / S::P, S::THREADS, S::SMEM_PEN>>>((double2 *)data_dev, batch, sign, tw); \
     }
     SPNS_FOR_EACH_LENGTH(SPNS_FFT1D)
 #undef SPNS_FFT1D
     cudaError_t e = cudaDeviceSynchronize();
-    if (e != cudaSuccess) return fail(h, SPNS_ERR_CUDA, "fft1d: %s", cudaGetErrorString(e));
+    if (e != cudaSuccess) return spns_fail(h, SPNS_ERR_CUDA, "fft1d: %s", cudaGetErrorString(e));
     return SPNS_OK;
 }

@@ -95,7 +95,7 @@ extern "C" int spns_energy_cascade_noalloc_f64(const void *uvw_dev, int Kx, int 
     const long long n = g.S0;
     const int blocks = (int)((n + 255) / 256 < 148 * 8 ? (n + 255) / 256 : 148 * 8);
     k_shell_sums<double><<<blocks, 256, sizeof(double) * 2 * nbins, st>>>(
-        g, (const cx<double> *)u, (const cx<double> *)(u + g.S0), (const cx<double> *)(u + 2 * g.S0), nbins - 1, bins,
+        g, (const cx<double> *)u, (const cx<double> *)(u + g.S0), (const cx<double> *)(u + 2 * g.S0), nullptr, nullptr, nullptr, nbins - 1, bins,
         bins + nbins);
     e = cudaGetLastError();
     if (e != cudaSuccess) return noalloc_fail(SPNS_ERR_CUDA, cudaGetErrorString(e));
