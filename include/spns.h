@@ -127,7 +127,8 @@ int spns_get_physical(spns_handle *h, double *uvw);
 
 /* Device-resident state for callers that keep their own device buffers:
  * pointers to the three spectral components (layout as spns_get_spectral,
- * element type double2 for SPNS_FP64). */
+ * element type double2 for SPNS_FP64; for SPNS_FP32_HILO the float2 high parts
+ * of the hi + lo pairs). */
 int spns_device_state(spns_handle *h, void **u, void **v, void **w);
 /* The CUDA stream all work of the handle is issued on (cudaStream_t). */
 int spns_stream(spns_handle *h, void **stream);

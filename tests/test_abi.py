@@ -34,3 +34,16 @@ def test_status_strings():
     L = hit.lib()
     assert L.spns_status_string(0) == b"ok"
     assert L.spns_status_string(-2) == b"unsupported size"
+
+
+def test_reference_driver_binds_only_declared_entry_points():
+    """The reference driver built against libspns resolves its solver calls to entry points of include/spns.h."""
+    import subprocess
+    exe = os.path.join(ROOT, "spns_b200", "dropin", "_build", "spns_hit_qa")
+    if not os.path.exists(exe):
+        pytest.skip("drop-in driver not built (needs the reference sources)")
+    out = subprocess.run(["nm", "-D", "--undefined-only", exe], capture_output=True, text=True, check=True).stdout
+    used = sorted(set(re.findall(r"\b(spns_[a-z0-9_]+)\b", out)))
+    assert used, "driver does not call libspns"
+    assert set(used) <= set(declared_symbols()), set(used) - set(declared_symbols())
+    assert "spns_step" in used and "spns_create" in used
