@@ -242,11 +242,19 @@ template <typename T, int P> struct SmRowMajor {
     cx<T> *base; int p;
     __device__ __forceinline__ cx<T> &at(int row) const { return base[row * P + p]; }
 };
-// Accessor: pencil-major [p][L+pad], one padding slot every 8 rows.
+// Accessor: pencil-major [p][PITCH] with an XOR swizzle of the low row bits
+// by the bits two places up (G = 8 rows of 16 bytes, or 16 rows of 8 bytes =
+// one 128-byte bank line).  It maps each aligned block of G rows onto itself,
+// so PITCH is L rounded up to a multiple of G.  For the strides of the
+// Stockham exchanges (R*Ns apart on write, L/R apart on read) it spreads a
+// quarter-warp (double) or half-warp (float) over distinct banks in nearly
+// every stage; a padding of one slot per 8 rows left some stages 2-way
+// conflicted (double) or all of them (float).
 template <typename T, int L> struct SmPencil {
     cx<T> *base;
-    static constexpr int PITCH = L + L / 8;
-    __device__ __forceinline__ cx<T> &at(int row) const { return base[row + (row >> 3)]; }
+    static constexpr int G = sizeof(cx<T>) == 16 ? 8 : 16;
+    static constexpr int PITCH = (L + G - 1) / G * G;
+    __device__ __forceinline__ cx<T> &at(int row) const { return base[row ^ ((row >> 2) & (G - 1))]; }
 };
 
 } // namespace spns

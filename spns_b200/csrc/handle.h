@@ -68,12 +68,19 @@ template <typename T, int L, int E_, int THR> struct ShapeT {
 #ifndef SPNS_Z_E
 #define SPNS_Z_E 12           // complex values per thread in the double z pass (3 pairs in registers)
 #endif
+#ifndef SPNS_Z_STAGE
+#define SPNS_Z_STAGE 1        // double z pass: stage the six input fields in shared memory
+#endif
+#ifndef SPNS_F32_Z_STAGE
+#define SPNS_F32_Z_STAGE 1
+#endif
 template <typename T> struct ShapeSel {
     static constexpr bool D = sizeof(T) == 8;
     static constexpr int K1_E = D ? 12 : SPNS_F32_K1_E, K1_T = D ? 256 : SPNS_F32_K1_T;
     static constexpr int K2_E = D ? 24 : SPNS_F32_K2_E, K2_T = D ? 256 : SPNS_F32_K2_T;
     static constexpr int K5_E = D ? 24 : SPNS_F32_K5_E, K5_T = D ? 128 : SPNS_F32_K5_T;
     static constexpr int Z_E = D ? SPNS_Z_E : SPNS_F32_Z_E, Z_T = D ? SPNS_Z_THREADS : SPNS_F32_Z_T;
+    static constexpr bool Z_STAGE = D ? SPNS_Z_STAGE : SPNS_F32_Z_STAGE;
 };
 template <typename T, int L> using ShapeK1 = ShapeT<T, L, ShapeSel<T>::K1_E, ShapeSel<T>::K1_T>;   // inverse x
 template <typename T, int L> using ShapeK2 = ShapeT<T, L, ShapeSel<T>::K2_E, ShapeSel<T>::K2_T>;   // inverse y (and forward y)

@@ -35,12 +35,14 @@ template <typename T> struct Passes {
     }
     template <int L, int MODE> static cudaError_t launch_k3(spns_handle *h, double *phys) {
         using S3 = Shape3<T, L, MODE>;
-        auto kern = spns::k3_z<T, L, S3::E, S3::P, MODE>;
-        cudaError_t e = spns_set_smem(kern, S3::SMEM);
+        constexpr bool STAGE = MODE == spns::MODE_ROT && ShapeSel<T>::Z_STAGE;
+        auto kern = spns::k3_z<T, L, S3::E, S3::P, MODE, STAGE>;
+        const size_t smem = S3::SMEM + (STAGE ? (size_t)S3::P * 6 * h->g.Kz * sizeof(C) : 0);
+        cudaError_t e = spns_set_smem(kern, smem);
         if (e != cudaSuccess) return e;
         const long long npen = (long long)h->g.Mx * h->g.My;
         dim3 grid((unsigned)((npen + S3::P - 1) / S3::P));
-        kern<<<grid, S3::THREADS, S3::SMEM, h->st>>>(h->g, (C *)h->B2, h->c, h->ds, phys, tw(h, L));
+        kern<<<grid, S3::THREADS, smem, h->st>>>(h->g, (C *)h->B2, h->c, h->ds, phys, tw(h, L));
         return cudaGetLastError();
     }
     template <int L, int MODE> static cudaError_t launch_k4(spns_handle *h) {

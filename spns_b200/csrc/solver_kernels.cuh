@@ -298,11 +298,26 @@ __device__ __forceinline__ void cfl_update(double (&mx)[4], double uu, double vv
     mx[3] = fmax(mx[3], s);
 }
 
+// Asynchronous global->shared copy of one complex element (LDGSTS; 16 B for
+// double, 8 B for float), completed per thread by commit/wait groups.
+template <typename T> __device__ __forceinline__ void cp_async_elem(cx<T> *smem_dst, const cx<T> *gsrc) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    if constexpr (sizeof(cx<T>) == 16) asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
+    else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 // Shared-memory slots of physical fields kept per pencil (rows of this thread only).
 // slots: 0 u, 1 v, 2 w, 3..5 conv_x,y,z, LES 6..11 a11, a12, a22, a13, a23, a33 (then t_ij)
 template <int MODE> struct K3Phys { static constexpr int N = MODE == MODE_ADV ? 6 : MODE == MODE_LES ? 12 : 0; };
 
-template <typename T, int L, int E, int P, int MODE>
+// STAGE (rotational form): the six input fields of the block's pencils are
+// copied into shared memory asynchronously at the start, in the order the
+// three pairs use them, so the loads of the second and third pairs overlap the
+// transforms of the first.  Dynamic shared memory then holds P*6*Kz extra
+// complex values after the exchange buffers.
+template <typename T, int L, int E, int P, int MODE, bool STAGE = false>
 __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ buf, StepConsts c, DevScalars *ds,
                                                    double *__restrict__ phys, const cx<T> *__restrict__ tw) {
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -350,11 +365,31 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
     } else if constexpr (MODE == MODE_ROT) {
         // pairs (u, w_x), (v, w_y), (w, w_z);  c = w x u  (= u.grad u + gradient)
         cx<T> A[E], B[E], C[E];
-        k3_load_pair<T, L, E>(A, F(0), false, F(3), false, g.Kz, sz, q, ok);
+        const cx<T> *src[6] = {F(0), F(1), F(2), F(3), F(4), F(5)};
+        if constexpr (STAGE) {
+            cx<T> *st = smc + P * SmPencil<T, L>::PITCH + (long long)p * 6 * g.Kz;
+#pragma unroll
+            for (int gp = 0; gp < 3; gp++) {
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int f = gp + 3 * h;        // (0,3), (1,4), (2,5)
+                    if (ok)
+                        for (int k = q; k < g.Kz; k += Q) cp_async_elem<T>(st + f * g.Kz + k, src[f] + k);
+                }
+                cp_async_commit();
+            }
+#pragma unroll
+            for (int f = 0; f < 6; f++) src[f] = st + f * g.Kz;
+            cp_async_wait<2>();
+            __syncthreads();
+        }
+        k3_load_pair<T, L, E>(A, src[0], false, src[3], false, g.Kz, sz, q, ok);
         fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(A, sm, q, tw);
-        k3_load_pair<T, L, E>(B, F(1), false, F(4), false, g.Kz, sz, q, ok);
+        if constexpr (STAGE) { cp_async_wait<1>(); __syncthreads(); }
+        k3_load_pair<T, L, E>(B, src[1], false, src[4], false, g.Kz, sz, q, ok);
         fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(B, sm, q, tw);
-        k3_load_pair<T, L, E>(C, F(2), false, F(5), false, g.Kz, sz, q, ok);
+        if constexpr (STAGE) { cp_async_wait<0>(); __syncthreads(); }
+        k3_load_pair<T, L, E>(C, src[2], false, src[5], false, g.Kz, sz, q, ok);
         fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(C, sm, q, tw);
 #pragma unroll
         for (int e = 0; e < E; e++) {
