@@ -44,12 +44,12 @@ def nu_for(N: int, eps: float = EPS) -> float:
     return (eta ** 4 * eps) ** (1.0 / 3.0)
 
 
-def box_args(N: int, self_adaptive: bool = True, nxy: int = 0):
+def box_args(N: int, self_adaptive: bool = True, nxy: int = 0, shape=None):
+    """Box of the forced DNS; `nxy` or `shape` (Nx, Ny, Nz) give reduced boxes for profiling."""
     from spns_b200.params import HitArgs
-    M = (3 * N) // 2
-    Nxy = nxy or N
-    Mxy = (3 * Nxy) // 2
-    return HitArgs(Nx=Nxy, Ny=Nxy, Nz=N, Mx=Mxy, My=Mxy, Mz=M, nu=nu_for(N), C_Smag=0.0, C_At=C_AT, Lx=1, Ly=1, Lz=1,
+    Nx, Ny, Nz = shape or (nxy or N, nxy or N, N)
+    M = lambda n: (3 * n) // 2  # noqa: E731
+    return HitArgs(Nx=Nx, Ny=Ny, Nz=Nz, Mx=M(Nx), My=M(Ny), Mz=M(Nz), nu=nu_for(N), C_Smag=0.0, C_At=C_AT, Lx=1, Ly=1, Lz=1,
                    omega_x=0.0, omega_y=0.0, omega_z=0.0, Nx_file=-1, Ny_file=-1, Nz_file=-1, isReLambda=False,
                    isInitialFieldFromBinaryFile=False, isInitialFieldFromASCIIFile=False, isNotCubic=False,
                    isRotating=False, isLES=False, isComplexConjugateCorrected=False, isSelfAdaptive=self_adaptive)
@@ -243,7 +243,8 @@ def run_gpu(args):
     from spns_b200.replicas import whole_job_rate
 
     N = args.n
-    a = box_args(N, nxy=args.nxy)
+    shape = tuple(int(v) for v in args.shape.split(",")) if args.shape else None
+    a = box_args(N, nxy=args.nxy, shape=shape)
     h = HIT(a, device=local, eps_forcing=EPS)
     U0 = seeded_spectral_field(a.Nx, a.Ny, a.Nz, kp=KP, seed=SEED + rank)
     h.set_compact(U0)
@@ -384,6 +385,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["spns", "reference"], default="spns")
     ap.add_argument("--n", type=int, default=N_BOX, help="retained modes per axis (default 512)")
+    ap.add_argument("--shape", default="",
+                    help="Nx,Ny,Nz of a reduced box for profiling one pass at its full FFT length "
+                         "(e.g. 64,512,64 runs the y passes at length 768)")
     ap.add_argument("--nxy", type=int, default=0,
                     help="retained modes along x and y (default: as --n); a small value gives a reduced box "
                          "that runs the same z-pass kernel, for profiling")
