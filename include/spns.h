@@ -135,6 +135,48 @@ int spns_stream(spns_handle *h, void **stream);
 /* Number of kernels issued by the last spns_step call (per step). */
 int spns_kernels_per_step(spns_handle *h, int *count);
 
+/* Device bytes a handle with these arguments allocates (state, history, work
+ * buffers, edge planes, twiddles), for admission against a memory budget.  The
+ * physical-field buffer of spns_get_physical is allocated later, on first use. */
+int spns_estimate_device_bytes(const spns_hit_args *args, size_t *bytes);
+
+/* Seeded initial field (no counterpart in the reference, which starts from its
+ * K41 draw or a file): complex Gaussian modes from Philox4x32-10 (key = seed,
+ * counter = compact mode index and draw number), projected onto k-perp, zero for
+ * |m_i| > (N_i-1)/2 and at k=0, Hermitian on kz=0, shells scaled to
+ * E(K) ~ K^4 exp(-2 (K/kp)^2) with total energy 3/2 urms^2.  Replaces the state;
+ * call spns_velocity_antitransform and spns_recalculate_timestep afterwards, as
+ * after spns_set_spectral. */
+int spns_seed_field(spns_handle *h, uint64_t seed, double kp, double urms);
+
+/* Asynchronous stepping for callers that keep many handles busy at once:
+ * spns_step_async enqueues nsteps steps on the handle's stream and returns;
+ * spns_query reports whether they have finished (*idle = 1); spns_synchronize
+ * waits and returns the status of the steps (as spns_step does). */
+int spns_step_async(spns_handle *h, int nsteps);
+int spns_query(spns_handle *h, int *idle);
+int spns_synchronize(spns_handle *h);
+
+/* Exact checkpoint of a handle: scalars (time, dt, kappa, iteration, ...),
+ * the state (hi and lo parts in FP32_HILO), R^{n-1} and, for the kappa scheme,
+ * u^{n-1}; loading it into a handle created with the same arguments resumes the
+ * run bit for bit. */
+int spns_checkpoint_bytes(spns_handle *h, size_t *bytes);
+int spns_checkpoint_save(spns_handle *h, void *buf, size_t bytes);
+int spns_checkpoint_load(spns_handle *h, const void *buf, size_t bytes);
+
+/* Ensembles (no counterpart in the reference, which runs one box per job):
+ * members of any sizes and precisions on one device advance together, one CUDA
+ * graph per step in which every member's step is an independent branch, so the
+ * kernels of small boxes run concurrently.  Each member's result equals the
+ * one it reaches stepped alone.  spns_ensemble_step synchronises and returns the
+ * first failing member's status (message from spns_ensemble_last_error). */
+typedef struct spns_ensemble spns_ensemble;
+int spns_ensemble_create(spns_handle *const *members, int n, spns_ensemble **out);
+int spns_ensemble_step(spns_ensemble *e, int nsteps);
+int spns_ensemble_destroy(spns_ensemble *e);
+const char *spns_ensemble_last_error(spns_ensemble *e);
+
 /* Per-kernel CUDA-event profile of the next max_steps calls of one step
  * (events recorded on the handle's stream between the kernels of a step). */
 int spns_profile_begin(spns_handle *h, int max_steps);

@@ -207,6 +207,7 @@ struct PrecOps {
     int (*shell_sums)(spns_handle *h);                        // E(K), Om(K) of u into h->bins
     int (*forcing_scale)(spns_handle *h, int last_eff, int nullify); // u *= FT[K]
     int (*conj_correction)(spns_handle *h);                   // kz=0 conjugate correction
+    int (*seed_draw)(spns_handle *h, unsigned long long seed, int lim_x, int lim_y, int lim_z); // Philox field, unscaled
 };
 extern const PrecOps spns_ops_f64;
 extern const PrecOps spns_ops_f32;

@@ -138,6 +138,15 @@ template <typename T> struct Passes {
         return SPNS_OK;
     }
 
+    static int seed_draw(spns_handle *h, unsigned long long seed, int lim_x, int lim_y, int lim_z) {
+        const long long n = h->g.S0;
+        const int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 16);
+        spns::k_seed_draw<T><<<blocks, 256, 0, h->st>>>(h->g, seed, lim_x, lim_y, lim_z, U(h, 0), U(h, 1), U(h, 2), Ulo(h, 0),
+                                                       Ulo(h, 1), Ulo(h, 2));
+        CKL();
+        return SPNS_OK;
+    }
+
     // Exact aliasing correction of the rotational form on the +-N/2 planes
     // (edge_kernels.cuh), added to the compact nonlinear term G held in B2.
     static int edge_correction(spns_handle *h) {
@@ -229,6 +238,6 @@ template <typename T> struct Passes {
     }
 
     static constexpr PrecOps ops() {
-        return PrecOps{&step_once, &run_velocity, &shell_sums, &forcing_scale, &conj_correction};
+        return PrecOps{&step_once, &run_velocity, &shell_sums, &forcing_scale, &conj_correction, &seed_draw};
     }
 };

@@ -917,6 +917,106 @@ __global__ void k_conj_correction(Geo g, cx<T> *u, cx<T> *v, cx<T> *w, cx<T> *ul
     }
 }
 
+// ===========================================================================
+// Seeded initial field on the device (no reference counterpart: the reference
+// starts from its K41 draw or a file).  Philox4x32-10 (Salmon, Moraes, Dror and
+// Shaw, "Parallel random numbers: as easy as 1, 2, 3", SC'11), key = seed,
+// counter = (compact mode index, draw number), so every mode draws its own
+// numbers and the field does not depend on the launch shape.
+// ===========================================================================
+struct Philox4 { unsigned x, y, z, w; };
+__host__ __device__ __forceinline__ Philox4 philox4x32_10(Philox4 c, unsigned k0, unsigned k1) {
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        const unsigned long long p0 = 0xD2511F53ull * c.x, p1 = 0xCD9E8D57ull * c.z;
+        Philox4 n;
+        n.x = (unsigned)(p1 >> 32) ^ c.y ^ k0;
+        n.y = (unsigned)p1;
+        n.z = (unsigned)(p0 >> 32) ^ c.w ^ k1;
+        n.w = (unsigned)p0;
+        c = n;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return c;
+}
+
+// Two standard normals from one Philox block: two 53-bit uniforms, Box-Muller.
+__device__ __forceinline__ void philox_normal2(unsigned long long idx, unsigned draw, unsigned long long seed, double &z0, double &z1) {
+    Philox4 c{(unsigned)idx, (unsigned)(idx >> 32), draw, 0u};
+    const Philox4 r = philox4x32_10(c, (unsigned)seed, (unsigned)(seed >> 32));
+    const double u0 = (double)(((unsigned long long)(r.x >> 5) << 26) | (r.y >> 6)) * 0x1.0p-53;
+    const double u1 = (double)(((unsigned long long)(r.z >> 5) << 26) | (r.w >> 6)) * 0x1.0p-53;
+    const double rad = sqrt(-2.0 * log(1.0 - u0));
+    double sn, cs;
+    sincospi(2.0 * u1, &sn, &cs);
+    z0 = rad * cs;
+    z1 = rad * sn;
+}
+
+// Complex Gaussian velocity of every retained mode, projected onto k-perp;
+// zero outside |m_i| <= lim_i and at k=0; on kz=0 the half with m1<0 (or
+// m1=0, m2<0) is the conjugate of its partner's draw.  Written as the state
+// (hi + lo split when lo is given).
+template <typename T>
+__global__ void k_seed_draw(Geo g, unsigned long long seed, int lim_x, int lim_y, int lim_z, cx<T> *u, cx<T> *v, cx<T> *w,
+                            cx<T> *ulo, cx<T> *vlo, cx<T> *wlo) {
+    const long long n = g.S0;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long long)gridDim.x * blockDim.x) {
+        const int kz = (int)(idx % g.Kz);
+        const long long t = idx / g.Kz;
+        const int ix = (int)(t % g.Kx), iy = (int)(t / g.Kx);
+        int m1 = ix <= g.hx ? ix : ix - g.Kx, m2 = iy <= g.hy ? iy : iy - g.Ky;
+        const double k1 = (double)g.sx * m1, k2 = (double)g.sy * m2, k3 = (double)g.sz * kz;
+        const double k2s = k1 * k1 + k2 * k2 + k3 * k3;
+        const bool keep = (m1 <= lim_x && -m1 <= lim_x && m2 <= lim_y && -m2 <= lim_y && kz <= lim_z && k2s > 0.0);
+        double re[3] = {0.0, 0.0, 0.0}, im[3] = {0.0, 0.0, 0.0};
+        if (keep) {
+            const bool mirror = kz == 0 && (m1 < 0 || (m1 == 0 && m2 < 0));
+            long long src = idx;
+            if (mirror) {
+                const int p1 = -m1, p2 = -m2;
+                src = ((long long)(p2 >= 0 ? p2 : p2 + g.Ky) * g.Kx + (p1 >= 0 ? p1 : p1 + g.Kx)) * g.Kz;
+            }
+            for (int c = 0; c < 3; c++) philox_normal2((unsigned long long)src, (unsigned)c, seed, re[c], im[c]);
+            const double kk[3] = {mirror ? -k1 : k1, mirror ? -k2 : k2, k3};
+            const double dr = (kk[0] * re[0] + kk[1] * re[1] + kk[2] * re[2]) / k2s;
+            const double di = (kk[0] * im[0] + kk[1] * im[1] + kk[2] * im[2]) / k2s;
+            for (int c = 0; c < 3; c++) { re[c] -= dr * kk[c]; im[c] -= di * kk[c]; }
+            if (mirror) for (int c = 0; c < 3; c++) im[c] = -im[c];
+        }
+        cx<T> *hs[3] = {u, v, w}, *ls[3] = {ulo, vlo, wlo};
+        for (int c = 0; c < 3; c++) {
+            const T hr = T(re[c]), hi = T(im[c]);
+            hs[c][idx] = mk<T>(hr, hi);
+            if (ulo) ls[c][idx] = mk<T>(T(re[c] - (double)hr), T(im[c] - (double)hi));
+        }
+    }
+}
+
+// Shell factors of the seeded field: target(K) = K^4 exp(-2 (K/kp)^2) on the
+// non-empty shells K >= 1, normalised to total energy 3/2 urms^2;
+// FT[K] = sqrt(target(K) / E(K)).  One block.
+static __global__ void k_seed_factors(const double *Ek, int Kmax, double kp, double urms, double *FT) {
+    __shared__ double tot;
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int K = 1; K <= Kmax; K++)
+            if (Ek[K] > 0.0) { const double x = (double)K / kp; s += (double)K * K * K * K * exp(-2.0 * x * x); }
+        tot = s;
+    }
+    __syncthreads();
+    for (int K = threadIdx.x; K <= Kmax; K += blockDim.x) {
+        double f = 0.0;
+        if (K >= 1 && Ek[K] > 0.0 && tot > 0.0) {
+            const double x = (double)K / kp;
+            const double target = (double)K * K * K * K * exp(-2.0 * x * x) * (1.5 * urms * urms) / tot;
+            f = sqrt(target / Ek[K]);
+        }
+        FT[K] = f;
+    }
+}
+
 // Direct DFT along one axis (initial-field transform of the input file; init only).
 // in: complex lines, out: complex lines; out[o][k] = sum_n in[o][n] * w^(k*n mod N).
 // Line l of `nl` lines starts at (l / inner)*outer_stride + (l % inner), element stride `es`.

@@ -205,6 +205,19 @@ static int file_init(spns_handle *h, const double *file_uvw, std::vector<double2
 // ---------------------------------------------------------------------------
 // Helpers for API calls
 // ---------------------------------------------------------------------------
+// Shell-factor buffers (target spectrum and factors) of at least n shells.
+static int ensure_forcing_capacity(spns_handle *h, int n) {
+    if (n <= h->forced_cap) return SPNS_OK;
+    CK(cudaStreamSynchronize(h->st));
+    if (h->forced) cudaFree(h->forced);
+    if (h->FT) cudaFree(h->FT);
+    h->forced = nullptr; h->FT = nullptr; h->forced_cap = 0;
+    CK(cudaMalloc(&h->forced, sizeof(double) * n));
+    CK(cudaMalloc(&h->FT, sizeof(double) * n));
+    h->forced_cap = n;
+    return SPNS_OK;
+}
+
 static int forcing_energy_cascade(spns_handle *h, const double *Forced, int last_input_rad, int nullify) {
     int r = spns_ops(h).shell_sums(h);
     if (r) return r;
@@ -212,14 +225,8 @@ static int forcing_energy_cascade(spns_handle *h, const double *Forced, int last
     k_totals<<<1, 1, 0, h->st>>>(h->bins, h->bins + nb, h->last_rad_max, h->ds, 0, 0.0);
     CKL();
     const int last_eff = std::min(last_input_rad, h->last_rad);
-    if (last_eff + 1 > h->forced_cap) {
-        if (h->forced) cudaFree(h->forced);
-        if (h->FT) cudaFree(h->FT);
-        h->forced = nullptr; h->FT = nullptr;
-        CK(cudaMalloc(&h->forced, sizeof(double) * (last_eff + 1)));
-        CK(cudaMalloc(&h->FT, sizeof(double) * (last_eff + 1)));
-        h->forced_cap = last_eff + 1;
-    }
+    r = ensure_forcing_capacity(h, last_eff + 1);
+    if (r) return r;
     CK(cudaMemcpyAsync(h->forced, Forced, sizeof(double) * (last_eff + 1), cudaMemcpyHostToDevice, h->st));
     k_forcing_factors<<<1, 256, 0, h->st>>>(h->bins, h->forced, last_eff, h->FT);
     CKL();
@@ -247,6 +254,66 @@ static int read_scalars(spns_handle *h, DevScalars *s) {
     CK(cudaMemcpyAsync(s, h->ds, sizeof(*s), cudaMemcpyDeviceToHost, h->st));
     CK(cudaStreamSynchronize(h->st));
     return SPNS_OK;
+}
+
+// Geometry of the true grid of a (possibly non-cubic) box (src/HIT_LES.h:31-36)
+// and the shell counts; SPNS_OK or an error status with the message recorded
+// in the handle-less error slot.
+static int box_geometry(const spns_hit_args &a, Geo &g, int &last_rad, int &last_rad_max) {
+    if (a.precision != SPNS_FP64 && a.precision != SPNS_FP32_HILO)
+        return spns_fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "unknown precision %d", a.precision);
+    if (a.Lx_factor < 1 || a.Ly_factor < 1 || a.Lz_factor < 1 || a.Nx < 2 || a.Ny < 2 || a.Nz < 2)
+        return spns_fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "invalid sizes or length factors");
+    const int ANx = actual_n(a.Nx, a.Lx_factor), ANy = actual_n(a.Ny, a.Ly_factor), ANz = actual_n(a.Nz, a.Lz_factor);
+    memset(&g, 0, sizeof(g));
+    g.hx = ANx / 2; g.hy = ANy / 2; g.hz = ANz / 2;
+    g.Kx = 2 * g.hx + 1; g.Ky = 2 * g.hy + 1; g.Kz = g.hz + 1;
+    g.Mx = actual_n(a.Mx, a.Lx_factor); g.My = actual_n(a.My, a.Ly_factor); g.Mz = actual_n(a.Mz, a.Lz_factor);
+    g.sx = a.Lx_factor; g.sy = a.Ly_factor; g.sz = a.Lz_factor;
+    g.S0 = (long long)g.Ky * g.Kx * g.Kz;
+    g.S1 = (long long)g.Ky * g.Mx * g.Kz;
+    g.S2 = (long long)g.My * g.Mx * g.Kz;
+    if (!spns_length_supported(g.Mx) || !spns_length_supported(g.My) || !spns_length_supported(g.Mz))
+        return spns_fail(nullptr, SPNS_ERR_UNSUPPORTED_SIZE, "FFT grid %dx%dx%d outside the compiled lengths", g.Mx, g.My, g.Mz);
+    if (2 * g.hx >= g.Mx || 2 * g.hy >= g.My || 2 * g.hz >= g.Mz)
+        return spns_fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "retained modes do not fit the FFT grid");
+    last_rad = std::min((a.Nx - 1) / 2, std::min((a.Ny - 1) / 2, (a.Nz - 1) / 2));
+    last_rad_max = (int)std::ceil(std::sqrt(1.0 * (a.Nx / 2) * (a.Nx / 2) + 1.0 * (a.Ny / 2) * (a.Ny / 2) + 1.0 * (a.Nz / 2) * (a.Nz / 2)));
+    return SPNS_OK;
+}
+
+// Device buffers of a handle (bytes), in the order spns_create allocates them.
+struct BufferPlan {
+    size_t state, lo, R, Up, Uplo, B1, B2, bins, edge, tw, scalars;
+    int nB1, nB2;
+    bool need_edge, edge_axis[3];
+    size_t total() const { return state + lo + R + Up + Uplo + B1 + B2 + bins + edge + tw + scalars; }
+};
+static BufferPlan buffer_plan(const spns_hit_args &a, const Geo &g, int last_rad_max) {
+    BufferPlan p;
+    memset(&p, 0, sizeof(p));
+    const size_t cs = a.precision == SPNS_FP64 ? sizeof(double2) : sizeof(float2);
+    const bool hilo = a.precision == SPNS_FP32_HILO;
+    const bool rot = !a.isLES && a.nonlinear_form != 2;
+    p.nB1 = rot ? 5 : 6;
+    p.nB2 = rot ? 6 : 9;
+    // planes k_i = +-h alias onto each other when M_i = 3 h_i (even number of retained modes)
+    p.edge_axis[0] = g.hx > 0 && g.Mx <= 3 * g.hx;
+    p.edge_axis[1] = g.hy > 0 && g.My <= 3 * g.hy;
+    p.edge_axis[2] = g.hz > 0 && g.Mz <= 3 * g.hz;
+    p.need_edge = rot && a.nonlinear_form == 0 && (p.edge_axis[0] || p.edge_axis[1] || p.edge_axis[2]);
+    p.state = cs * 3 * (size_t)g.S0;
+    p.lo = hilo ? p.state : 0;
+    p.R = p.state;
+    p.Up = a.isSelfAdaptive ? p.state : 0;
+    p.Uplo = a.isSelfAdaptive && hilo ? p.state : 0;
+    p.B1 = cs * p.nB1 * (size_t)g.S1;
+    p.B2 = cs * p.nB2 * (size_t)g.S2;
+    p.bins = sizeof(double) * 2 * (size_t)(last_rad_max + 1);
+    p.edge = p.need_edge ? cs * 8 * (size_t)std::max((long long)g.My * g.Mz, std::max((long long)g.Mx * g.Mz, (long long)g.Mx * g.My)) : 0;
+    p.tw = cs * ((size_t)g.Mx + g.My + g.Mz);
+    p.scalars = sizeof(DevScalars);
+    return p;
 }
 
 static void free_handle(spns_handle *h) {
@@ -285,42 +352,25 @@ int spns_create(const spns_hit_args *args, const double *file_uvw, spns_handle *
     spns_handle *h = nullptr;
     if (!args || !out) return spns_fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "null argument");
     *out = nullptr;
-    if (args->precision != SPNS_FP64 && args->precision != SPNS_FP32_HILO)
-        return spns_fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "unknown precision %d", args->precision);
-    if (args->Lx_factor < 1 || args->Ly_factor < 1 || args->Lz_factor < 1 || args->Nx < 2 || args->Ny < 2 || args->Nz < 2)
-        return spns_fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "invalid sizes or length factors");
     if (args->isInitialFieldFromFile && !file_uvw) return spns_fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "file initial field requested without data");
+    Geo g0;
+    int last_rad = 0, last_rad_max = 0;
+    int rc = box_geometry(*args, g0, last_rad, last_rad_max);
+    if (rc) return rc;
     h = new spns_handle();
     h->a = *args;
     h->prec = args->precision;
     h->csz = h->prec == SPNS_FP64 ? sizeof(double2) : sizeof(float2);
     const spns_hit_args &a = h->a;
-    int rc;
     {
         cudaError_t e = cudaSetDevice(a.device);
         if (e != cudaSuccess) { spns_fail(nullptr, SPNS_ERR_CUDA, "cudaSetDevice(%d): %s", a.device, cudaGetErrorString(e)); delete h; return SPNS_ERR_CUDA; }
     }
-    // geometry (true grid of a non-cubic box, src/HIT_LES.h:31-36)
-    Geo &g = h->g;
-    const int ANx = actual_n(a.Nx, a.Lx_factor), ANy = actual_n(a.Ny, a.Ly_factor), ANz = actual_n(a.Nz, a.Lz_factor);
-    const int AMx = actual_n(a.Mx, a.Lx_factor), AMy = actual_n(a.My, a.Ly_factor), AMz = actual_n(a.Mz, a.Lz_factor);
-    g.hx = ANx / 2; g.hy = ANy / 2; g.hz = ANz / 2;
-    g.Kx = 2 * g.hx + 1; g.Ky = 2 * g.hy + 1; g.Kz = g.hz + 1;
-    g.Mx = AMx; g.My = AMy; g.Mz = AMz;
-    g.sx = a.Lx_factor; g.sy = a.Ly_factor; g.sz = a.Lz_factor;
-    g.S0 = (long long)g.Ky * g.Kx * g.Kz;
-    g.S1 = (long long)g.Ky * g.Mx * g.Kz;
-    g.S2 = (long long)g.My * g.Mx * g.Kz;
-    if (!spns_length_supported(g.Mx) || !spns_length_supported(g.My) || !spns_length_supported(g.Mz)) {
-        rc = spns_fail(nullptr, SPNS_ERR_UNSUPPORTED_SIZE, "FFT grid %dx%dx%d outside the compiled lengths", g.Mx, g.My, g.Mz);
-        delete h; return rc;
-    }
-    if (2 * g.hx >= g.Mx || 2 * g.hy >= g.My || 2 * g.hz >= g.Mz) {
-        rc = spns_fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "retained modes do not fit the FFT grid");
-        delete h; return rc;
-    }
-    h->last_rad = std::min((a.Nx - 1) / 2, std::min((a.Ny - 1) / 2, (a.Nz - 1) / 2));
-    h->last_rad_max = (int)std::ceil(std::sqrt(1.0 * (a.Nx / 2) * (a.Nx / 2) + 1.0 * (a.Ny / 2) * (a.Ny / 2) + 1.0 * (a.Nz / 2) * (a.Nz / 2)));
+    h->g = g0;
+    const Geo &g = h->g;
+    const int AMx = g.Mx, AMy = g.My, AMz = g.Mz;
+    h->last_rad = last_rad;
+    h->last_rad_max = last_rad_max;
     const double PI_ = 3.141592653589793238462643;
     StepConsts &c = h->c;
     memset(&c, 0, sizeof(c));
@@ -348,26 +398,18 @@ int spns_create(const spns_hit_args *args, const double *file_uvw, spns_handle *
     // device memory
     auto cleanup = [&](int code) { free_handle(h); return code; };
     if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) return cleanup(spns_fail(nullptr, SPNS_ERR_CUDA, "stream creation failed"));
-    const bool rot = !a.isLES && a.nonlinear_form != 2;
-    h->nB1 = rot ? 5 : 6;
-    h->nB2 = rot ? 6 : 9;
-    // planes k_i = +-h alias onto each other when M_i = 3 h_i (even number of retained modes)
-    h->edge_axis[0] = g.hx > 0 && g.Mx <= 3 * g.hx;
-    h->edge_axis[1] = g.hy > 0 && g.My <= 3 * g.hy;
-    h->edge_axis[2] = g.hz > 0 && g.Mz <= 3 * g.hz;
-    const bool need_edge = rot && a.nonlinear_form == 0 && (h->edge_axis[0] || h->edge_axis[1] || h->edge_axis[2]);
-    const size_t cs = h->csz;
-    const size_t s0 = cs * 3 * g.S0;
+    const BufferPlan bp = buffer_plan(a, g, h->last_rad_max);
+    h->nB1 = bp.nB1;
+    h->nB2 = bp.nB2;
+    for (int i = 0; i < 3; i++) h->edge_axis[i] = bp.edge_axis[i];
+    const size_t s0 = bp.state;
     const bool hilo = h->prec == SPNS_FP32_HILO;
-    bool okm = cudaMalloc(&h->ds, sizeof(DevScalars)) == cudaSuccess && cudaMalloc(&h->U, s0) == cudaSuccess &&
-               (!hilo || cudaMalloc(&h->Ulo, s0) == cudaSuccess) && cudaMalloc(&h->R, s0) == cudaSuccess &&
-               (!a.isSelfAdaptive || cudaMalloc(&h->Up, s0) == cudaSuccess) &&
-               (!a.isSelfAdaptive || !hilo || cudaMalloc(&h->Uplo, s0) == cudaSuccess) &&
-               cudaMalloc(&h->B1, cs * h->nB1 * g.S1) == cudaSuccess &&
-               cudaMalloc(&h->B2, cs * h->nB2 * g.S2) == cudaSuccess &&
-               cudaMalloc(&h->bins, sizeof(double) * 2 * (h->last_rad_max + 1)) == cudaSuccess &&
-               (!need_edge || cudaMalloc(&h->edge, cs * 8 *
-                                         (size_t)std::max((long long)g.My * g.Mz, std::max((long long)g.Mx * g.Mz, (long long)g.Mx * g.My))) == cudaSuccess);
+    bool okm = cudaMalloc(&h->ds, bp.scalars) == cudaSuccess && cudaMalloc(&h->U, bp.state) == cudaSuccess &&
+               (!bp.lo || cudaMalloc(&h->Ulo, bp.lo) == cudaSuccess) && cudaMalloc(&h->R, bp.R) == cudaSuccess &&
+               (!bp.Up || cudaMalloc(&h->Up, bp.Up) == cudaSuccess) &&
+               (!bp.Uplo || cudaMalloc(&h->Uplo, bp.Uplo) == cudaSuccess) &&
+               cudaMalloc(&h->B1, bp.B1) == cudaSuccess && cudaMalloc(&h->B2, bp.B2) == cudaSuccess &&
+               cudaMalloc(&h->bins, bp.bins) == cudaSuccess && (!bp.edge || cudaMalloc(&h->edge, bp.edge) == cudaSuccess);
     if (!okm) { cudaGetLastError(); return cleanup(spns_fail(nullptr, SPNS_ERR_OUT_OF_MEMORY, "device allocation failed")); }
     for (int L : {g.Mx, g.My, g.Mz})
         if (!h->tw.count(L)) {
@@ -429,6 +471,8 @@ int spns_destroy(spns_handle *h) {
     return SPNS_OK;
 }
 
+int spns_step_async(spns_handle *h, int nsteps);
+
 // One step as a replay of a captured CUDA graph.  The kernel arguments hold
 // the state-buffer pointers, which the kappa scheme swaps every step, so one
 // graph is kept per parity.  Capture issues no work; the first (uncaptured)
@@ -455,12 +499,8 @@ static int step_graph(spns_handle *h) {
 
 int spns_step(spns_handle *h, int nsteps) {
     if (!h || nsteps < 0) return SPNS_ERR_INVALID_ARGUMENT;
-    for (int i = 0; i < nsteps; i++) {
-        const bool profiling = h->prof_steps < h->prof_cap_steps;
-        const bool warm = h->kernels_per_step > 0;   // a first step has run uncaptured
-        int r = (h->use_graphs && warm && !profiling) ? step_graph(h) : spns_ops(h).step_once(h);
-        if (r) return r;
-    }
+    int r = spns_step_async(h, nsteps);
+    if (r) return r;
     return check_flags(h);
 }
 
@@ -667,7 +707,288 @@ const char *spns_profile_kernel_name(spns_handle *h, int i) {
     return h->prof_names[i].c_str();
 }
 
+int spns_estimate_device_bytes(const spns_hit_args *args, size_t *bytes) {
+    if (!args || !bytes) return spns_fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "null argument");
+    Geo g;
+    int last_rad = 0, last_rad_max = 0;
+    int rc = box_geometry(*args, g, last_rad, last_rad_max);
+    if (rc) return rc;
+    *bytes = buffer_plan(*args, g, last_rad_max).total();
+    return SPNS_OK;
+}
+
+int spns_seed_field(spns_handle *h, uint64_t seed, double kp, double urms) {
+    if (!h || !(kp > 0.0) || !(urms >= 0.0)) return h ? spns_fail(h, SPNS_ERR_INVALID_ARGUMENT, "invalid kp or urms") : SPNS_ERR_INVALID_ARGUMENT;
+    const spns_hit_args &a = h->a;
+    const int lim_x = (actual_n(a.Nx, a.Lx_factor) - 1) / 2, lim_y = (actual_n(a.Ny, a.Ly_factor) - 1) / 2,
+              lim_z = (actual_n(a.Nz, a.Lz_factor) - 1) / 2;
+    int r = spns_ops(h).seed_draw(h, (unsigned long long)seed, lim_x, lim_y, lim_z);
+    if (r) return r;
+    r = spns_ops(h).shell_sums(h);
+    if (r) return r;
+    r = ensure_forcing_capacity(h, h->last_rad_max + 1);
+    if (r) return r;
+    k_seed_factors<<<1, 256, 0, h->st>>>(h->bins, h->last_rad_max, kp, urms, h->FT);
+    CKL();
+    r = spns_ops(h).forcing_scale(h, h->last_rad_max, 0);
+    if (r) return r;
+    CK(cudaStreamSynchronize(h->st));
+    return SPNS_OK;
+}
+
+// Enqueue nsteps steps on the handle's stream and return (no synchronisation,
+// no status check); spns_synchronize completes them.
+int spns_step_async(spns_handle *h, int nsteps) {
+    if (!h || nsteps < 0) return SPNS_ERR_INVALID_ARGUMENT;
+    for (int i = 0; i < nsteps; i++) {
+        const bool profiling = h->prof_steps < h->prof_cap_steps;
+        const bool warm = h->kernels_per_step > 0;   // a first step has run uncaptured
+        int r = (h->use_graphs && warm && !profiling) ? step_graph(h) : spns_ops(h).step_once(h);
+        if (r) return r;
+    }
+    return SPNS_OK;
+}
+
+int spns_synchronize(spns_handle *h) {
+    if (!h) return SPNS_ERR_INVALID_ARGUMENT;
+    return check_flags(h);
+}
+
+int spns_query(spns_handle *h, int *idle) {
+    if (!h || !idle) return SPNS_ERR_INVALID_ARGUMENT;
+    const cudaError_t e = cudaStreamQuery(h->st);
+    if (e == cudaSuccess) { *idle = 1; return SPNS_OK; }
+    if (e == cudaErrorNotReady) { cudaGetLastError(); *idle = 0; return SPNS_OK; }
+    return spns_fail(h, SPNS_ERR_CUDA, "cudaStreamQuery: %s", cudaGetErrorString(e));
+}
+
+// ---------------------------------------------------------------------------
+// Checkpoint: header, scalars, state (hi [+lo]), R^{n-1}, u^{n-1} (kappa).
+// ---------------------------------------------------------------------------
+struct CheckpointHeader {
+    char magic[8];                 // "SPNSCKP1"
+    int precision, isSelfAdaptive, isLES, nonlinear_form;
+    int Kx, Ky, Kz, Mx, My, Mz, sx, sy, sz;
+    long long S0;
+    unsigned long long bytes;      // total size including this header
+};
+
+static void checkpoint_layout(const spns_handle *h, size_t &field, size_t &total) {
+    field = h->csz * 3 * (size_t)h->g.S0;
+    const int nstate = (h->prec == SPNS_FP32_HILO ? 2 : 1) * (h->a.isSelfAdaptive ? 2 : 1) + 1;  // u(,lo)(,up(,uplo)), R
+    total = sizeof(CheckpointHeader) + sizeof(DevScalars) + field * nstate;
+}
+
+int spns_checkpoint_bytes(spns_handle *h, size_t *bytes) {
+    if (!h || !bytes) return SPNS_ERR_INVALID_ARGUMENT;
+    size_t field, total;
+    checkpoint_layout(h, field, total);
+    *bytes = total;
+    return SPNS_OK;
+}
+
+int spns_checkpoint_save(spns_handle *h, void *buf, size_t bytes) {
+    if (!h || !buf) return SPNS_ERR_INVALID_ARGUMENT;
+    size_t field, total;
+    checkpoint_layout(h, field, total);
+    if (bytes < total) return spns_fail(h, SPNS_ERR_INVALID_ARGUMENT, "checkpoint buffer of %zu bytes, %zu needed", bytes, total);
+    CheckpointHeader hd;
+    memset(&hd, 0, sizeof(hd));
+    memcpy(hd.magic, "SPNSCKP1", 8);
+    hd.precision = h->prec; hd.isSelfAdaptive = h->a.isSelfAdaptive; hd.isLES = h->a.isLES; hd.nonlinear_form = h->a.nonlinear_form;
+    hd.Kx = h->g.Kx; hd.Ky = h->g.Ky; hd.Kz = h->g.Kz; hd.Mx = h->g.Mx; hd.My = h->g.My; hd.Mz = h->g.Mz;
+    hd.sx = h->g.sx; hd.sy = h->g.sy; hd.sz = h->g.sz; hd.S0 = h->g.S0; hd.bytes = total;
+    char *p = (char *)buf;
+    memcpy(p, &hd, sizeof(hd));
+    p += sizeof(hd);
+    CK(cudaMemcpyAsync(p, h->ds, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->st));
+    p += sizeof(DevScalars);
+    void *parts[5] = {h->U, h->Ulo, h->R, h->Up, h->Uplo};
+    for (void *src : parts) {
+        if (!src) continue;
+        CK(cudaMemcpyAsync(p, src, field, cudaMemcpyDeviceToHost, h->st));
+        p += field;
+    }
+    CK(cudaStreamSynchronize(h->st));
+    return SPNS_OK;
+}
+
+int spns_checkpoint_load(spns_handle *h, const void *buf, size_t bytes) {
+    if (!h || !buf) return SPNS_ERR_INVALID_ARGUMENT;
+    size_t field, total;
+    checkpoint_layout(h, field, total);
+    if (bytes < sizeof(CheckpointHeader)) return spns_fail(h, SPNS_ERR_INVALID_ARGUMENT, "checkpoint too short");
+    CheckpointHeader hd;
+    memcpy(&hd, buf, sizeof(hd));
+    if (memcmp(hd.magic, "SPNSCKP1", 8) != 0) return spns_fail(h, SPNS_ERR_INVALID_ARGUMENT, "not a libspns checkpoint");
+    if (hd.bytes != total || bytes < total || hd.precision != h->prec || hd.isSelfAdaptive != h->a.isSelfAdaptive ||
+        hd.Kx != h->g.Kx || hd.Ky != h->g.Ky || hd.Kz != h->g.Kz || hd.Mx != h->g.Mx || hd.My != h->g.My || hd.Mz != h->g.Mz ||
+        hd.sx != h->g.sx || hd.sy != h->g.sy || hd.sz != h->g.sz)
+        return spns_fail(h, SPNS_ERR_INVALID_ARGUMENT, "checkpoint does not match this box (size, precision or scheme)");
+    const char *p = (const char *)buf + sizeof(hd);
+    CK(cudaMemcpyAsync(h->ds, p, sizeof(DevScalars), cudaMemcpyHostToDevice, h->st));
+    p += sizeof(DevScalars);
+    void *parts[5] = {h->U, h->Ulo, h->R, h->Up, h->Uplo};
+    for (void *dst : parts) {
+        if (!dst) continue;
+        CK(cudaMemcpyAsync(dst, p, field, cudaMemcpyHostToDevice, h->st));
+        p += field;
+    }
+    CK(cudaStreamSynchronize(h->st));
+    return SPNS_OK;
+}
+
 } // extern "C"
+
+// ---------------------------------------------------------------------------
+// Ensembles: one CUDA graph advances every member by one step.  Each member's
+// step is an independent branch of the graph (forked from and joined to the
+// ensemble's stream), so kernels of different boxes run concurrently.  Graphs
+// are kept per pattern of state-buffer parities (the kappa scheme swaps its
+// buffers every step; the graph bakes the pointers in).
+// ---------------------------------------------------------------------------
+struct spns_ensemble {
+    std::vector<spns_handle *> m;
+    cudaStream_t st = nullptr;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
+    std::map<std::vector<bool>, cudaGraphExec_t> graphs;
+    std::string err;
+    int device = 0;
+};
+
+static std::vector<bool> ensemble_parity(const spns_ensemble *e) {
+    std::vector<bool> p(e->m.size());
+    for (size_t i = 0; i < e->m.size(); i++) p[i] = e->m[i]->U != e->m[i]->U0;
+    return p;
+}
+
+static void ensemble_free(spns_ensemble *e) {
+    if (!e) return;
+    for (auto &kv : e->graphs) cudaGraphExecDestroy(kv.second);
+    for (auto ev : e->join) if (ev) cudaEventDestroy(ev);
+    if (e->fork) cudaEventDestroy(e->fork);
+    if (e->st) cudaStreamDestroy(e->st);
+    delete e;
+}
+
+#define ECK(call)                                                                                  \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) {                                                                   \
+            char b_[512];                                                                          \
+            snprintf(b_, sizeof(b_), "%s failed: %s", #call, cudaGetErrorString(e_));             \
+            e->err = b_;                                                                           \
+            return SPNS_ERR_CUDA;                                                                  \
+        }                                                                                          \
+    } while (0)
+
+extern "C" int spns_ensemble_create(spns_handle *const *members, int n, spns_ensemble **out) {
+    if (!members || n < 1 || !out) return spns_fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "invalid ensemble arguments");
+    *out = nullptr;
+    const int dev = members[0]->a.device;
+    for (int i = 0; i < n; i++) {
+        if (!members[i]) return spns_fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "null ensemble member %d", i);
+        if (members[i]->a.device != dev) return spns_fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "ensemble members on different devices");
+        for (int j = 0; j < i; j++)
+            if (members[j] == members[i]) return spns_fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "member %d listed twice", i);
+    }
+    spns_ensemble *e = new spns_ensemble();
+    e->m.assign(members, members + n);
+    e->device = dev;
+    e->join.assign(n, nullptr);
+    bool ok = cudaSetDevice(dev) == cudaSuccess && cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) == cudaSuccess;
+    for (int i = 0; ok && i < n; i++) ok = cudaEventCreateWithFlags(&e->join[i], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) { ensemble_free(e); return spns_fail(nullptr, SPNS_ERR_CUDA, "ensemble stream/event creation failed"); }
+    *out = e;
+    return SPNS_OK;
+}
+
+extern "C" int spns_ensemble_destroy(spns_ensemble *e) {
+    if (!e) return SPNS_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(e->device);
+    cudaStreamSynchronize(e->st);
+    ensemble_free(e);
+    return SPNS_OK;
+}
+
+extern "C" const char *spns_ensemble_last_error(spns_ensemble *e) { return e ? e->err.c_str() : ""; }
+
+// Advances every member by nsteps steps.  Members that have not yet run a step
+// run their first one uncaptured (each on its own stream, concurrently); the
+// rest are replays of the ensemble graph.  Synchronises and checks every
+// member's status at the end; the first failing member is named in the error.
+extern "C" int spns_ensemble_step(spns_ensemble *e, int nsteps) {
+    if (!e || nsteps < 0) return SPNS_ERR_INVALID_ARGUMENT;
+    ECK(cudaSetDevice(e->device));
+    const int n = (int)e->m.size();
+    // order the ensemble's stream after the members' earlier work
+    for (int i = 0; i < n; i++) {
+        ECK(cudaEventRecord(e->join[i], e->m[i]->st));
+        ECK(cudaStreamWaitEvent(e->st, e->join[i], 0));
+    }
+    for (int s = 0; s < nsteps; s++) {
+        bool cold = false;
+        for (auto *h : e->m) cold = cold || h->kernels_per_step == 0;
+        if (cold) {
+            ECK(cudaEventRecord(e->fork, e->st));
+            for (int i = 0; i < n; i++) {
+                spns_handle *h = e->m[i];
+                ECK(cudaStreamWaitEvent(h->st, e->fork, 0));
+                int r = spns_ops(h).step_once(h);
+                if (r) { e->err = "member " + std::to_string(i) + ": " + h->err; return r; }
+                ECK(cudaEventRecord(e->join[i], h->st));
+                ECK(cudaStreamWaitEvent(e->st, e->join[i], 0));
+            }
+            continue;
+        }
+        const std::vector<bool> par = ensemble_parity(e);
+        auto it = e->graphs.find(par);
+        if (it == e->graphs.end()) {
+            std::vector<void *> U(n), Up(n), Ulo(n), Uplo(n);
+            for (int i = 0; i < n; i++) { U[i] = e->m[i]->U; Up[i] = e->m[i]->Up; Ulo[i] = e->m[i]->Ulo; Uplo[i] = e->m[i]->Uplo; }
+            cudaGraph_t gr = nullptr;
+            ECK(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
+            int r = SPNS_OK;
+            cudaError_t ce = cudaEventRecord(e->fork, e->st);
+            for (int i = 0; i < n && r == SPNS_OK && ce == cudaSuccess; i++) {
+                spns_handle *h = e->m[i];
+                ce = cudaStreamWaitEvent(h->st, e->fork, 0);
+                if (ce != cudaSuccess) break;
+                r = spns_ops(h).step_once(h);
+                if (r) { e->err = "member " + std::to_string(i) + ": " + h->err; break; }
+                ce = cudaEventRecord(e->join[i], h->st);
+                if (ce == cudaSuccess) ce = cudaStreamWaitEvent(e->st, e->join[i], 0);
+            }
+            cudaError_t ee = cudaStreamEndCapture(e->st, &gr);
+            for (int i = 0; i < n; i++) { e->m[i]->U = U[i]; e->m[i]->Up = Up[i]; e->m[i]->Ulo = Ulo[i]; e->m[i]->Uplo = Uplo[i]; }
+            if (r) { if (gr) cudaGraphDestroy(gr); return r; }
+            if (ce != cudaSuccess || ee != cudaSuccess) {
+                if (gr) cudaGraphDestroy(gr);
+                e->err = std::string("ensemble capture failed: ") + cudaGetErrorString(ce != cudaSuccess ? ce : ee);
+                return SPNS_ERR_CUDA;
+            }
+            cudaGraphExec_t ex = nullptr;
+            ce = cudaGraphInstantiate(&ex, gr, 0);
+            cudaGraphDestroy(gr);
+            if (ce != cudaSuccess) { e->err = std::string("ensemble graph instantiation failed: ") + cudaGetErrorString(ce); return SPNS_ERR_CUDA; }
+            it = e->graphs.emplace(par, ex).first;
+        }
+        ECK(cudaGraphLaunch(it->second, e->st));
+        for (auto *h : e->m)
+            if (h->a.isSelfAdaptive) { std::swap(h->U, h->Up); std::swap(h->Ulo, h->Uplo); }
+    }
+    // order the members' later work after the ensemble's, then check every member
+    ECK(cudaEventRecord(e->fork, e->st));
+    for (auto *h : e->m) ECK(cudaStreamWaitEvent(h->st, e->fork, 0));
+    ECK(cudaStreamSynchronize(e->st));
+    for (int i = 0; i < n; i++) {
+        int r = check_flags(e->m[i]);
+        if (r) { e->err = "member " + std::to_string(i) + ": " + e->m[i]->err; return r; }
+    }
+    return SPNS_OK;
+}
 
 // ---------------------------------------------------------------------------
 // Test building block: batched 1-D FFT of contiguous lines (one line per

@@ -96,3 +96,79 @@ def energy_spectrum(U: np.ndarray, Nx: int, Ny: int, Nz: int, scale=(1, 1, 1), n
     e = 0.5 * np.sum(np.abs(U) ** 2, axis=0) * w
     n = nbins or int(K.max()) + 1
     return np.bincount(K.ravel(), weights=e.ravel(), minlength=n)[:n]
+
+
+# ---------------------------------------------------------------------------
+# Philox4x32-10 seeded field: the host restatement of the device generator of
+# libspns (spns_seed_field), used to check it.  Philox4x32-10 is the published
+# counter-based generator of Salmon, Moraes, Dror and Shaw (SC'11).
+# ---------------------------------------------------------------------------
+_M32 = np.uint64(0xFFFFFFFF)
+
+
+def philox4x32_10(c0, c1, c2, c3, k0, k1):
+    """Vectorised Philox4x32-10 over uint64 arrays holding 32-bit words."""
+    c0, c1, c2, c3 = (np.asarray(v, dtype=np.uint64) & _M32 for v in (c0, c1, c2, c3))
+    k0 = np.uint64(int(k0) & 0xFFFFFFFF)
+    k1 = np.uint64(int(k1) & 0xFFFFFFFF)
+    for _ in range(10):
+        p0 = np.uint64(0xD2511F53) * c0
+        p1 = np.uint64(0xCD9E8D57) * c2
+        c0, c1, c2, c3 = (((p1 >> np.uint64(32)) ^ c1 ^ k0) & _M32, p1 & _M32,
+                          ((p0 >> np.uint64(32)) ^ c3 ^ k1) & _M32, p0 & _M32)
+        k0 = (k0 + np.uint64(0x9E3779B9)) & _M32
+        k1 = (k1 + np.uint64(0xBB67AE85)) & _M32
+    return c0, c1, c2, c3
+
+
+def _philox_normals(idx, draw, seed):
+    r = philox4x32_10(idx & 0xFFFFFFFF, idx >> np.uint64(32), np.full_like(idx, draw), np.zeros_like(idx),
+                      seed & 0xFFFFFFFF, seed >> 32)
+    u0 = ((r[0] >> np.uint64(5)) * np.uint64(1 << 26) + (r[1] >> np.uint64(6))).astype(np.float64) * 2.0 ** -53
+    u1 = ((r[2] >> np.uint64(5)) * np.uint64(1 << 26) + (r[3] >> np.uint64(6))).astype(np.float64) * 2.0 ** -53
+    rad = np.sqrt(-2.0 * np.log(1.0 - u0))
+    return rad * np.cos(2.0 * np.pi * u1), rad * np.sin(2.0 * np.pi * u1)
+
+
+def philox_spectral_field(Nx: int, Ny: int, Nz: int, kp: float = 4.0, seed: int = 0, urms: float = 1.0,
+                          scale=(1, 1, 1)) -> np.ndarray:
+    """The field spns_seed_field writes, computed on the host ([3][Ky][Kx][Kz] complex128)."""
+    hx, hy, hz = Nx // 2, Ny // 2, Nz // 2
+    Kx, Ky, Kz = 2 * hx + 1, 2 * hy + 1, hz + 1
+    sx, sy, sz = scale
+    lim_x, lim_y, lim_z = (Nx - 1) // 2, (Ny - 1) // 2, (Nz - 1) // 2
+    iy, ix, kz = np.meshgrid(np.arange(Ky), np.arange(Kx), np.arange(Kz), indexing="ij")
+    m1 = np.where(ix <= hx, ix, ix - Kx)
+    m2 = np.where(iy <= hy, iy, iy - Ky)
+    k1, k2, k3 = float(sx) * m1, float(sy) * m2, float(sz) * kz
+    k2s = k1 * k1 + k2 * k2 + k3 * k3
+    keep = (np.abs(m1) <= lim_x) & (np.abs(m2) <= lim_y) & (kz <= lim_z) & (k2s > 0)
+    mirror = (kz == 0) & ((m1 < 0) | ((m1 == 0) & (m2 < 0)))
+    p1, p2 = -m1, -m2
+    src_mirror = ((np.where(p2 >= 0, p2, p2 + Ky) * Kx + np.where(p1 >= 0, p1, p1 + Kx)) * Kz)
+    idx = (iy * Kx + ix) * Kz + kz
+    src = np.where(mirror, src_mirror, idx).astype(np.uint64)
+    re, im = [], []
+    for c in range(3):
+        a, b = _philox_normals(src, c, int(seed))
+        re.append(a)
+        im.append(b)
+    kk = [np.where(mirror, -k1, k1), np.where(mirror, -k2, k2), k3]
+    safe = np.where(k2s > 0, k2s, 1.0)
+    dr = (kk[0] * re[0] + kk[1] * re[1] + kk[2] * re[2]) / safe
+    di = (kk[0] * im[0] + kk[1] * im[1] + kk[2] * im[2]) / safe
+    U = np.zeros((3, Ky, Kx, Kz), dtype=np.complex128)
+    for c in range(3):
+        r = re[c] - dr * kk[c]
+        i = im[c] - di * kk[c]
+        i = np.where(mirror, -i, i)
+        U[c] = np.where(keep, r + 1j * i, 0.0)
+    K, w = shell_index(Nx, Ny, Nz, scale)
+    last_rad_max = int(np.ceil(np.sqrt((sx * hx) ** 2 + (sy * hy) ** 2 + (sz * hz) ** 2)))
+    e = 0.5 * np.sum(np.abs(U) ** 2, axis=0) * w
+    E = np.bincount(K.ravel(), weights=e.ravel(), minlength=last_rad_max + 1)[:last_rad_max + 1]
+    Ks = np.arange(last_rad_max + 1, dtype=np.float64)
+    shape = np.where((Ks >= 1) & (E > 0), Ks ** 4 * np.exp(-2.0 * (Ks / kp) ** 2), 0.0)
+    target = shape * (1.5 * urms * urms) / shape.sum()
+    fac = np.sqrt(np.divide(target, E, out=np.zeros_like(target), where=E > 0))
+    return U * fac[np.minimum(K, last_rad_max)][None]

@@ -30,7 +30,9 @@ EXPORTED_SYMBOLS = (
     "spns_spectral_dims", "spns_physical_dims", "spns_get_spectral", "spns_set_spectral", "spns_get_physical",
     "spns_device_state", "spns_stream", "spns_kernels_per_step", "spns_last_error", "spns_status_string",
     "spns_fft1d_batch_f64", "spns_profile_begin", "spns_profile_read", "spns_profile_kernel_name",
-    "spns_energy_cascade_noalloc_f64",
+    "spns_energy_cascade_noalloc_f64", "spns_estimate_device_bytes", "spns_seed_field", "spns_step_async",
+    "spns_query", "spns_synchronize", "spns_checkpoint_bytes", "spns_checkpoint_save", "spns_checkpoint_load",
+    "spns_ensemble_create", "spns_ensemble_step", "spns_ensemble_destroy", "spns_ensemble_last_error",
 )
 
 
@@ -113,6 +115,20 @@ def lib():
         L.spns_profile_kernel_name.argtypes = [vp, i]
         L.spns_profile_kernel_name.restype = C.c_char_p
         L.spns_energy_cascade_noalloc_f64.argtypes = [vp, i, i, i, i, i, i, dp, i, dp, vp]
+        sz = C.c_size_t
+        L.spns_estimate_device_bytes.argtypes = [C.POINTER(HitArgsC), C.POINTER(sz)]
+        L.spns_seed_field.argtypes = [vp, C.c_uint64, d, d]
+        L.spns_step_async.argtypes = [vp, i]
+        L.spns_query.argtypes = [vp, ip]
+        L.spns_synchronize.argtypes = [vp]
+        L.spns_checkpoint_bytes.argtypes = [vp, C.POINTER(sz)]
+        L.spns_checkpoint_save.argtypes = [vp, vp, sz]
+        L.spns_checkpoint_load.argtypes = [vp, vp, sz]
+        L.spns_ensemble_create.argtypes = [C.POINTER(vp), i, C.POINTER(vp)]
+        L.spns_ensemble_step.argtypes = [vp, i]
+        L.spns_ensemble_destroy.argtypes = [vp]
+        L.spns_ensemble_last_error.argtypes = [vp]
+        L.spns_ensemble_last_error.restype = C.c_char_p
         _lib = L
     return _lib
 
@@ -129,6 +145,40 @@ def fft1d_batch_f64(dev_ptr: int, n: int, batch: int, sign: int) -> None:
         raise SpnsError(st, L.spns_last_error(None).decode())
 
 
+def make_args_c(args: HitArgs, *, precision: int = SPNS_FP64, device: int = 0, k41_ranks: int = 1,
+                fixed_dt: float = 0.0, eps_forcing: float = 0.0, eps_kmin: int = 1, eps_kmax: int = 2,
+                nonlinear_form: int = 0) -> HitArgsC:
+    """spns_hit_args of a HIT constructor call (src/HIT_LES.h:23-29) plus the extensions."""
+    a = HitArgsC()
+    for f in ("Nx", "Ny", "Nz", "Mx", "My", "Mz", "Nx_file", "Ny_file", "Nz_file"):
+        setattr(a, f, int(getattr(args, f)))
+    a.Lx_factor, a.Ly_factor, a.Lz_factor = int(args.Lx), int(args.Ly), int(args.Lz)
+    for f in ("nu", "C_Smag", "C_At", "omega_x", "omega_y", "omega_z"):
+        setattr(a, f, float(getattr(args, f)))
+    a.isReLambda = int(args.isReLambda)
+    a.isInitialFieldFromFile = int(args.is_file_init)
+    a.isNotCubic = int(args.isNotCubic)
+    a.isRotating = int(args.isRotating)
+    a.isLES = int(args.isLES)
+    a.isComplexConjugateCorrected = int(args.isComplexConjugateCorrected)
+    a.isSelfAdaptive = int(args.isSelfAdaptive)
+    a.precision, a.device, a.k41_ranks = int(precision), int(device), int(k41_ranks)
+    a.fixed_dt, a.eps_forcing = float(fixed_dt), float(eps_forcing)
+    a.eps_kmin, a.eps_kmax = int(eps_kmin), int(eps_kmax)
+    a.nonlinear_form = int(nonlinear_form)
+    return a
+
+
+def estimate_device_bytes(args: HitArgs, **options) -> int:
+    """Device bytes a handle with these arguments allocates (admission against a budget)."""
+    L = lib()
+    n = C.c_size_t()
+    st = L.spns_estimate_device_bytes(C.byref(make_args_c(args, **options)), C.byref(n))
+    if st != 0:
+        raise SpnsError(st, L.spns_last_error(None).decode())
+    return int(n.value)
+
+
 class HIT:
     """GPU solver with the interface of the reference class ``HIT`` (src/HIT_LES.h:21-246)."""
 
@@ -136,23 +186,9 @@ class HIT:
                  device: int = 0, k41_ranks: int = 1, fixed_dt: float = 0.0, eps_forcing: float = 0.0,
                  eps_kmin: int = 1, eps_kmax: int = 2, nonlinear_form: int = 0):
         L = lib()
-        a = HitArgsC()
-        for f in ("Nx", "Ny", "Nz", "Mx", "My", "Mz", "Nx_file", "Ny_file", "Nz_file"):
-            setattr(a, f, int(getattr(args, f)))
-        a.Lx_factor, a.Ly_factor, a.Lz_factor = int(args.Lx), int(args.Ly), int(args.Lz)
-        for f in ("nu", "C_Smag", "C_At", "omega_x", "omega_y", "omega_z"):
-            setattr(a, f, float(getattr(args, f)))
-        a.isReLambda = int(args.isReLambda)
-        a.isInitialFieldFromFile = int(args.is_file_init)
-        a.isNotCubic = int(args.isNotCubic)
-        a.isRotating = int(args.isRotating)
-        a.isLES = int(args.isLES)
-        a.isComplexConjugateCorrected = int(args.isComplexConjugateCorrected)
-        a.isSelfAdaptive = int(args.isSelfAdaptive)
-        a.precision, a.device, a.k41_ranks = int(precision), int(device), int(k41_ranks)
-        a.fixed_dt, a.eps_forcing = float(fixed_dt), float(eps_forcing)
-        a.eps_kmin, a.eps_kmax = int(eps_kmin), int(eps_kmax)
-        a.nonlinear_form = int(nonlinear_form)
+        a = make_args_c(args, precision=precision, device=device, k41_ranks=k41_ranks, fixed_dt=fixed_dt,
+                        eps_forcing=eps_forcing, eps_kmin=eps_kmin, eps_kmax=eps_kmax, nonlinear_form=nonlinear_form)
+        self.precision = int(precision)
         self.args = args
         fp = None
         if args.is_file_init:
@@ -304,7 +340,66 @@ class HIT:
         arr = np.frombuffer(buf, dtype=np.float32, count=nk.value * ns.value).reshape(ns.value, nk.value).copy()
         return names, arr
 
+    # --- extensions: seeded field, asynchronous stepping, checkpoints ---
+    def seed_field(self, seed: int, kp: float = 4.0, urms: float = 1.0):
+        """Seeded Philox field (spns_seed_field); then refresh the grid velocity and the time step."""
+        self._ck(self._L.spns_seed_field(self._h, int(seed) & 0xFFFFFFFFFFFFFFFF, float(kp), float(urms)))
+        self.Recalculate_Velocity_Antitransform()
+        self.Recalculate_TimeStep()
+
+    def step_async(self, nsteps: int = 1):
+        self._ck(self._L.spns_step_async(self._h, int(nsteps)))
+
+    def query(self) -> bool:
+        idle = C.c_int()
+        self._ck(self._L.spns_query(self._h, C.byref(idle)))
+        return bool(idle.value)
+
+    def synchronize(self):
+        self._ck(self._L.spns_synchronize(self._h))
+
+    def checkpoint_save(self) -> bytes:
+        n = C.c_size_t()
+        self._ck(self._L.spns_checkpoint_bytes(self._h, C.byref(n)))
+        buf = (C.c_char * n.value)()
+        self._ck(self._L.spns_checkpoint_save(self._h, buf, n.value))
+        return bytes(buf)
+
+    def checkpoint_load(self, data: bytes):
+        buf = (C.c_char * len(data)).from_buffer_copy(data)
+        self._ck(self._L.spns_checkpoint_load(self._h, buf, len(data)))
+
     def stream_handle(self) -> int:
         p = C.c_void_p()
         self._ck(self._L.spns_stream(self._h, C.byref(p)))
         return p.value or 0
+
+
+class Ensemble:
+    """Members advanced together, one CUDA graph per step (spns_ensemble_*)."""
+
+    def __init__(self, members):
+        L = lib()
+        self.members = list(members)
+        arr = (C.c_void_p * len(self.members))(*[m._h for m in self.members])
+        e = C.c_void_p()
+        st = L.spns_ensemble_create(arr, len(self.members), C.byref(e))
+        if st != 0:
+            raise SpnsError(st, L.spns_last_error(None).decode())
+        self._e, self._L = e, L
+
+    def step(self, nsteps: int = 1):
+        st = self._L.spns_ensemble_step(self._e, int(nsteps))
+        if st != 0:
+            raise SpnsError(st, self._L.spns_ensemble_last_error(self._e).decode())
+
+    def close(self):
+        if getattr(self, "_e", None):
+            self._L.spns_ensemble_destroy(self._e)
+            self._e = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
