@@ -202,6 +202,104 @@ def cpu_baseline_block(threads: int, n_sample: int = 96, steps: int = 3):
                        f"the reference layout needs ~200 GB of host RAM at N={N_BOX}")}
 
 
+def _timed_steps(h, n: int) -> float:
+    """Wall seconds of n steps through the public API (graph replays, synchronised)."""
+    t0 = time.perf_counter()
+    h.New_Fractional_Step_Method(n)
+    return time.perf_counter() - t0
+
+
+def ensemble_block(local: int, n_boxes: int = 64, steps: int = 500, seed: int = 7):
+    """64 LES boxes of uneven size advanced together (one CUDA graph per step, FP32 form).
+
+    Grids uniform in {32,48,64,96}^3 (FFT 48..144), Cs uniform in [0.10, 0.20],
+    nu=1e-4, per-instance Philox seeds with k_p=3, u_rms=1, CFL dt (C_At=0.5).
+    The sequential baselines step each box alone (its own CUDA graph per step),
+    in the same FP32 form and in the plain FP64 form, timed over `probe` steps
+    and scaled to `steps`."""
+    import numpy as np
+    from spns_b200.hit import HIT, Ensemble, SPNS_FP64, SPNS_FP32_HILO
+    from spns_b200.serving import box_args as sbox
+    rng = np.random.default_rng(seed)
+    specs = [(int(rng.choice([32, 48, 64, 96])), float(rng.uniform(0.10, 0.20)), int(rng.integers(0, 2 ** 63)))
+             for _ in range(n_boxes)]
+    members = []
+    for N, cs, sd in specs:
+        h = HIT(sbox(N, nu=1e-4, C_Smag=cs), precision=SPNS_FP32_HILO, device=local)
+        h.seed_field(sd, 3.0, 1.0)
+        members.append(h)
+    ens = Ensemble(members)
+    ens.step(3)                                   # first step uncaptured, then graph capture
+    t0 = time.perf_counter()
+    ens.step(steps)
+    t_ens = time.perf_counter() - t0
+    ens.close()
+    for h in members:
+        h.close()
+    probe = 20
+    seq = {}
+    for prec, name in ((SPNS_FP32_HILO, "fp32_hilo"), (SPNS_FP64, "fp64")):
+        tot = 0.0
+        for N, cs, sd in specs:
+            h = HIT(sbox(N, nu=1e-4, C_Smag=cs), precision=prec, device=local)
+            h.seed_field(sd, 3.0, 1.0)
+            h.New_Fractional_Step_Method(3)
+            tot += _timed_steps(h, probe) / probe * steps
+            h.close()
+        seq[name] = tot
+    box_steps = n_boxes * steps
+    return {"boxes": n_boxes, "steps_each": steps, "dtype": "FP32 compensated form",
+            "grids": {str(N): sum(1 for s_ in specs if s_[0] == N) for N in (32, 48, 64, 96)},
+            "box_steps_per_s": box_steps / t_ens, "wall_s": t_ens,
+            "sequential_fp32_box_steps_per_s": box_steps / seq["fp32_hilo"],
+            "sequential_plain_fp64_box_steps_per_s": box_steps / seq["fp64"],
+            "speedup_vs_sequential_fp32": seq["fp32_hilo"] / t_ens,
+            "speedup_vs_sequential_plain_fp64": seq["fp64"] / t_ens,
+            "how": "one CUDA graph per step with every box's step as a parallel branch; sequential baselines "
+                   f"timed over {probe} steps per box and scaled to {steps}"}
+
+
+def serving_block(local: int, n_requests: int = 40, rate: float = 20.0, seed: int = 11, budget_gb: float = 150.0):
+    """Served workload: Poisson arrivals of LES/DNS runs, continuous batching.
+
+    Grids {32,64,128,256}^3 with weights 0.4/0.3/0.2/0.1, steps uniform in
+    [200, 2000], LES (Cs in [0.10, 0.20], nu in [1e-4, 1e-3]) or DNS (nu in
+    [1e-3, 1e-2]) with equal odds, seeded k_p=3 spectra, FP32 form, 150 GB HBM
+    budget.  The sequential plain-path baseline runs the same requests one at
+    a time in FP64: each (grid, LES/DNS) class is timed alone over `probe`
+    steps and the per-request times are summed."""
+    from spns_b200.hit import HIT, SPNS_FP64
+    from spns_b200.serving import GpuBackend, Server, summarize, synthetic_workload
+    reqs = synthetic_workload(n_requests, rate=rate, seed=seed)
+    srv = Server(GpuBackend(device=local), budget_bytes=int(budget_gb * 1e9), chunk=25)
+    t0 = time.perf_counter()
+    res = srv.run(reqs)
+    makespan = time.perf_counter() - t0
+    out = summarize(res, makespan)
+    probe = 20
+    per_step = {}
+    for r in reqs:
+        key = (r.args.Nx, r.args.isLES)
+        if key in per_step:
+            continue
+        h = HIT(r.args, precision=SPNS_FP64, device=local)
+        h.seed_field(r.seed, r.kp, r.urms)
+        h.New_Fractional_Step_Method(3)
+        per_step[key] = _timed_steps(h, probe) / probe
+        h.close()
+    seq = sum(per_step[(r.args.Nx, r.args.isLES)] * r.nsteps for r in reqs if res[r.rid].status == "done")
+    out.update({
+        "workload": f"{n_requests} requests, Poisson {rate:g}/s, grids 32/64/128/256 (0.4/0.3/0.2/0.1), "
+                    "steps U[200,2000], LES or DNS, FP32 form, 150 GB budget",
+        "peak_budget_used_gb": srv.peak_used / 1e9,
+        "sequential_plain_fp64_solves_per_s": out["done"] / seq if seq > 0 else None,
+        "speedup_vs_sequential_plain_fp64": (out["solves_per_s"] * seq / out["done"]) if out["done"] else None,
+        "how": "latency = completion - arrival (wall clock); sequential plain path = the same requests one at a "
+               f"time in FP64, per-class step time from {probe} timed steps",
+    })
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", 0))
     if rank != 0:
@@ -370,6 +468,10 @@ def run_gpu(args):
                      "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                      "algorithmic_bytes": bytes_per[dom]},
     }
+    if not args.no_ensemble:
+        line["ensemble"] = ensemble_block(local)
+    if not args.no_serving:
+        line["serving"] = serving_block(local, n_requests=args.serving_requests)
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_block(os.cpu_count() or 1)
     print(json.dumps(line), flush=True)
@@ -394,6 +496,9 @@ def main():
     ap.add_argument("--ref-sample-n", type=int, default=96)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true", help="skip the compensated FP32 form's extra line field")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-box LES ensemble field")
+    ap.add_argument("--no-serving", action="store_true", help="skip the served-workload field")
+    ap.add_argument("--serving-requests", type=int, default=40)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

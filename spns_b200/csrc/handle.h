@@ -181,8 +181,9 @@ int spns_fail(spns_handle *h, int code, const char *fmt, ...);
     default: return spns_fail(h, SPNS_ERR_UNSUPPORTED_SIZE, "FFT length %d is not compiled", Lval); \
     }
 
-// Twiddle table w_L^m = exp(-2 pi i m / L), computed in extended precision.
-template <typename T> inline void *spns_make_twiddles(int L) {
+// Twiddle table w_L^m = exp(-2 pi i m / L), computed in extended precision;
+// allocated in stream order on `st` (no device-wide synchronisation).
+template <typename T> inline void *spns_make_twiddles(int L, cudaStream_t st) {
     std::vector<spns::cx<T>> t(L);
     for (int m = 0; m < L; m++) {
         long double ang = 2.0L * 3.14159265358979323846264338327950288L * (long double)m / (long double)L;
@@ -190,8 +191,12 @@ template <typename T> inline void *spns_make_twiddles(int L) {
         t[m].y = (T)(-sinl(ang));
     }
     void *d = nullptr;
-    if (cudaMalloc(&d, sizeof(spns::cx<T>) * L) != cudaSuccess) return nullptr;
-    if (cudaMemcpy(d, t.data(), sizeof(spns::cx<T>) * L, cudaMemcpyHostToDevice) != cudaSuccess) { cudaFree(d); return nullptr; }
+    if (cudaMallocAsync(&d, sizeof(spns::cx<T>) * L, st) != cudaSuccess) return nullptr;
+    if (cudaMemcpyAsync(d, t.data(), sizeof(spns::cx<T>) * L, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+        cudaFreeAsync(d, st);
+        return nullptr;
+    }
     return d;
 }
 

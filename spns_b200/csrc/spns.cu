@@ -141,8 +141,8 @@ static int file_init(spns_handle *h, const double *file_uvw, std::vector<double2
     CK(cudaMalloc(&d_b, sizeof(double2) * nspec));
     int maxn = std::max(nx, std::max(ny, nz));
     CK(cudaMalloc(&d_k, sizeof(int) * maxn));
-    twx = (double2 *)spns_make_twiddles<double>(nx); twy = (double2 *)spns_make_twiddles<double>(ny);
-    twz = (double2 *)spns_make_twiddles<double>(nz);
+    twx = (double2 *)spns_make_twiddles<double>(nx, h->st); twy = (double2 *)spns_make_twiddles<double>(ny, h->st);
+    twz = (double2 *)spns_make_twiddles<double>(nz, h->st);
     if (!twx || !twy || !twz) return spns_fail(h, SPNS_ERR_OUT_OF_MEMORY, "twiddle allocation failed");
     std::vector<int> kk(maxn);
     for (int i = 0; i < maxn; i++) kk[i] = i;
@@ -163,7 +163,8 @@ static int file_init(spns_handle *h, const double *file_uvw, std::vector<double2
         CKL();
         CK(cudaMemcpy(spec.data() + c * nspec, d_a, sizeof(double2) * nspec, cudaMemcpyDeviceToHost));
     }
-    cudaFree(d_in); cudaFree(d_a); cudaFree(d_b); cudaFree(d_k); cudaFree(twx); cudaFree(twy); cudaFree(twz);
+    cudaFree(d_in); cudaFree(d_a); cudaFree(d_b); cudaFree(d_k);
+    cudaFreeAsync(twx, h->st); cudaFreeAsync(twy, h->st); cudaFreeAsync(twz, h->st);
     const double normf = (double)nf;
     for (auto &z : spec) { z.x /= normf; z.y /= normf; }
     // Calculate_Ek_init_file over every file mode (expanded wavenumbers k = L*m)
@@ -208,12 +209,11 @@ static int file_init(spns_handle *h, const double *file_uvw, std::vector<double2
 // Shell-factor buffers (target spectrum and factors) of at least n shells.
 static int ensure_forcing_capacity(spns_handle *h, int n) {
     if (n <= h->forced_cap) return SPNS_OK;
-    CK(cudaStreamSynchronize(h->st));
-    if (h->forced) cudaFree(h->forced);
-    if (h->FT) cudaFree(h->FT);
+    if (h->forced) cudaFreeAsync(h->forced, h->st);
+    if (h->FT) cudaFreeAsync(h->FT, h->st);
     h->forced = nullptr; h->FT = nullptr; h->forced_cap = 0;
-    CK(cudaMalloc(&h->forced, sizeof(double) * n));
-    CK(cudaMalloc(&h->FT, sizeof(double) * n));
+    CK(cudaMallocAsync(&h->forced, sizeof(double) * n, h->st));
+    CK(cudaMallocAsync(&h->FT, sizeof(double) * n, h->st));
     h->forced_cap = n;
     return SPNS_OK;
 }
@@ -318,10 +318,12 @@ static BufferPlan buffer_plan(const spns_hit_args &a, const Geo &g, int last_rad
 
 static void free_handle(spns_handle *h) {
     if (!h) return;
-    cudaFree(h->ds); cudaFree(h->U); cudaFree(h->Ulo); cudaFree(h->R); cudaFree(h->Up); cudaFree(h->Uplo);
-    cudaFree(h->B1); cudaFree(h->B2);
-    cudaFree(h->bins); cudaFree(h->FT); cudaFree(h->forced); cudaFree(h->phys); cudaFree(h->edge);
-    for (auto &kv : h->tw) cudaFree(kv.second);
+    // stream-ordered frees: no device-wide synchronisation, so other handles'
+    // work in flight (a serving loop) keeps running while this one is released
+    void *bufs[] = {h->ds, h->U, h->Ulo, h->R, h->Up, h->Uplo, h->B1, h->B2, h->bins, h->FT, h->forced, h->phys, h->edge};
+    for (void *b : bufs)
+        if (b) cudaFreeAsync(b, h->st);
+    for (auto &kv : h->tw) cudaFreeAsync(kv.second, h->st);
     for (auto ev : h->prof_ev) cudaEventDestroy(ev);
     for (auto &gx : h->graph) if (gx) cudaGraphExecDestroy(gx);
     if (h->st) cudaStreamDestroy(h->st);
@@ -404,28 +406,28 @@ int spns_create(const spns_hit_args *args, const double *file_uvw, spns_handle *
     for (int i = 0; i < 3; i++) h->edge_axis[i] = bp.edge_axis[i];
     const size_t s0 = bp.state;
     const bool hilo = h->prec == SPNS_FP32_HILO;
-    bool okm = cudaMalloc(&h->ds, bp.scalars) == cudaSuccess && cudaMalloc(&h->U, bp.state) == cudaSuccess &&
-               (!bp.lo || cudaMalloc(&h->Ulo, bp.lo) == cudaSuccess) && cudaMalloc(&h->R, bp.R) == cudaSuccess &&
-               (!bp.Up || cudaMalloc(&h->Up, bp.Up) == cudaSuccess) &&
-               (!bp.Uplo || cudaMalloc(&h->Uplo, bp.Uplo) == cudaSuccess) &&
-               cudaMalloc(&h->B1, bp.B1) == cudaSuccess && cudaMalloc(&h->B2, bp.B2) == cudaSuccess &&
-               cudaMalloc(&h->bins, bp.bins) == cudaSuccess && (!bp.edge || cudaMalloc(&h->edge, bp.edge) == cudaSuccess);
+    // stream-ordered allocations (no device-wide synchronisation with other handles' work)
+    auto amalloc = [&](void **p, size_t n) { return n == 0 || cudaMallocAsync(p, n, h->st) == cudaSuccess; };
+    bool okm = amalloc((void **)&h->ds, bp.scalars) && amalloc(&h->U, bp.state) && amalloc(&h->Ulo, bp.lo) &&
+               amalloc(&h->R, bp.R) && amalloc(&h->Up, bp.Up) && amalloc(&h->Uplo, bp.Uplo) && amalloc(&h->B1, bp.B1) &&
+               amalloc(&h->B2, bp.B2) && amalloc((void **)&h->bins, bp.bins) && amalloc(&h->edge, bp.edge);
     if (!okm) { cudaGetLastError(); return cleanup(spns_fail(nullptr, SPNS_ERR_OUT_OF_MEMORY, "device allocation failed")); }
     for (int L : {g.Mx, g.My, g.Mz})
         if (!h->tw.count(L)) {
-            void *t = hilo ? spns_make_twiddles<float>(L) : spns_make_twiddles<double>(L);
+            void *t = hilo ? spns_make_twiddles<float>(L, h->st) : spns_make_twiddles<double>(L, h->st);
             if (!t) return cleanup(spns_fail(nullptr, SPNS_ERR_OUT_OF_MEMORY, "twiddle allocation failed"));
             h->tw[L] = t;
         }
-    cudaMemset(h->R, 0, s0);
-    if (h->Up) cudaMemset(h->Up, 0, s0);
-    if (h->Uplo) cudaMemset(h->Uplo, 0, s0);
     DevScalars s0v;
     memset(&s0v, 0, sizeof(s0v));
     s0v.nu = a.nu;
     s0v.kappa = 0.5;
-    if (cudaMemcpy(h->ds, &s0v, sizeof(s0v), cudaMemcpyHostToDevice) != cudaSuccess)
-        return cleanup(spns_fail(nullptr, SPNS_ERR_CUDA, "scalar upload failed"));
+    bool okz = cudaMemsetAsync(h->R, 0, s0, h->st) == cudaSuccess &&
+               (!h->Up || cudaMemsetAsync(h->Up, 0, s0, h->st) == cudaSuccess) &&
+               (!h->Uplo || cudaMemsetAsync(h->Uplo, 0, s0, h->st) == cudaSuccess) &&
+               cudaMemcpyAsync(h->ds, &s0v, sizeof(s0v), cudaMemcpyHostToDevice, h->st) == cudaSuccess &&
+               cudaStreamSynchronize(h->st) == cudaSuccess;
+    if (!okz) return cleanup(spns_fail(nullptr, SPNS_ERR_CUDA, "buffer initialisation failed"));
 
     // initial field
     std::vector<double2> uvw;
@@ -639,7 +641,7 @@ int spns_set_spectral(spns_handle *h, const double *uvw) {
 int spns_get_physical(spns_handle *h, double *uvw) {
     if (!h || !uvw) return SPNS_ERR_INVALID_ARGUMENT;
     const long long n3 = (long long)h->g.Mx * h->g.My * h->g.Mz;
-    if (!h->phys) CK(cudaMalloc(&h->phys, sizeof(double) * 3 * n3));
+    if (!h->phys) CK(cudaMallocAsync(&h->phys, sizeof(double) * 3 * n3, h->st));
     int r = spns_ops(h).run_velocity(h, h->phys);
     if (r) return r;
     CK(cudaMemcpyAsync(uvw, h->phys, sizeof(double) * 3 * n3, cudaMemcpyDeviceToHost, h->st));
@@ -1031,7 +1033,7 @@ extern "C" int spns_fft1d_batch_f64(void *data_dev, int n, int batch, int sign) 
     cudaGetDevice(&dev);
     auto key = std::make_pair(dev, n);
     if (!tws.count(key)) {
-        double2 *t = (double2 *)spns_make_twiddles<double>(n);
+        double2 *t = (double2 *)spns_make_twiddles<double>(n, 0);
         if (!t) return spns_fail(h, SPNS_ERR_OUT_OF_MEMORY, "twiddle allocation failed");
         tws[key] = t;
     }
