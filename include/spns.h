@@ -63,6 +63,9 @@ typedef struct spns_hit_args {
                                 1: rotational without the correction (equal only while the
                                 +-N/2 modes carry no energy); 2: advective, 12 inverse
                                 transforms, the reference's arithmetic */
+    int stream_priority;     /* CUDA stream priority of the handle's work (0 = default;
+                                lower values run first, clamped to the device's range).
+                                A serving loop gives short runs precedence this way. */
 } spns_hit_args;
 
 typedef struct spns_handle spns_handle;

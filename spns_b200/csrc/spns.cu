@@ -399,7 +399,13 @@ int spns_create(const spns_hit_args *args, const double *file_uvw, spns_handle *
 
     // device memory
     auto cleanup = [&](int code) { free_handle(h); return code; };
-    if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) return cleanup(spns_fail(nullptr, SPNS_ERR_CUDA, "stream creation failed"));
+    {
+        int least = 0, greatest = 0;
+        cudaDeviceGetStreamPriorityRange(&least, &greatest);
+        const int prio = std::max(greatest, std::min(least, a.stream_priority));
+        if (cudaStreamCreateWithPriority(&h->st, cudaStreamNonBlocking, prio) != cudaSuccess)
+            return cleanup(spns_fail(nullptr, SPNS_ERR_CUDA, "stream creation failed"));
+    }
     const BufferPlan bp = buffer_plan(a, g, h->last_rad_max);
     h->nB1 = bp.nB1;
     h->nB2 = bp.nB2;

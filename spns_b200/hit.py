@@ -58,6 +58,7 @@ class HitArgsC(C.Structure):
         ("precision", C.c_int), ("device", C.c_int), ("k41_ranks", C.c_int),
         ("fixed_dt", C.c_double), ("eps_forcing", C.c_double),
         ("eps_kmin", C.c_int), ("eps_kmax", C.c_int), ("nonlinear_form", C.c_int),
+        ("stream_priority", C.c_int),
     ]
 
 
@@ -147,7 +148,7 @@ def fft1d_batch_f64(dev_ptr: int, n: int, batch: int, sign: int) -> None:
 
 def make_args_c(args: HitArgs, *, precision: int = SPNS_FP64, device: int = 0, k41_ranks: int = 1,
                 fixed_dt: float = 0.0, eps_forcing: float = 0.0, eps_kmin: int = 1, eps_kmax: int = 2,
-                nonlinear_form: int = 0) -> HitArgsC:
+                nonlinear_form: int = 0, stream_priority: int = 0) -> HitArgsC:
     """spns_hit_args of a HIT constructor call (src/HIT_LES.h:23-29) plus the extensions."""
     a = HitArgsC()
     for f in ("Nx", "Ny", "Nz", "Mx", "My", "Mz", "Nx_file", "Ny_file", "Nz_file"):
@@ -166,6 +167,7 @@ def make_args_c(args: HitArgs, *, precision: int = SPNS_FP64, device: int = 0, k
     a.fixed_dt, a.eps_forcing = float(fixed_dt), float(eps_forcing)
     a.eps_kmin, a.eps_kmax = int(eps_kmin), int(eps_kmax)
     a.nonlinear_form = int(nonlinear_form)
+    a.stream_priority = int(stream_priority)
     return a
 
 
@@ -184,10 +186,11 @@ class HIT:
 
     def __init__(self, args: HitArgs, file_uvw: Optional[np.ndarray] = None, *, precision: int = SPNS_FP64,
                  device: int = 0, k41_ranks: int = 1, fixed_dt: float = 0.0, eps_forcing: float = 0.0,
-                 eps_kmin: int = 1, eps_kmax: int = 2, nonlinear_form: int = 0):
+                 eps_kmin: int = 1, eps_kmax: int = 2, nonlinear_form: int = 0, stream_priority: int = 0):
         L = lib()
         a = make_args_c(args, precision=precision, device=device, k41_ranks=k41_ranks, fixed_dt=fixed_dt,
-                        eps_forcing=eps_forcing, eps_kmin=eps_kmin, eps_kmax=eps_kmax, nonlinear_form=nonlinear_form)
+                        eps_forcing=eps_forcing, eps_kmin=eps_kmin, eps_kmax=eps_kmax, nonlinear_form=nonlinear_form,
+                        stream_priority=stream_priority)
         self.precision = int(precision)
         self.args = args
         fp = None

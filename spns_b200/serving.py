@@ -77,9 +77,9 @@ class GpuBackend:
         from .hit import estimate_device_bytes
         return estimate_device_bytes(req.args, precision=req.precision, device=self.device)
 
-    def create(self, req: SolveRequest):
+    def create(self, req: SolveRequest, priority: int = 0):
         from .hit import HIT
-        h = HIT(req.args, precision=req.precision, device=self.device)
+        h = HIT(req.args, precision=req.precision, device=self.device, stream_priority=priority)
         if req.init is not None:
             h.checkpoint_load(req.init)
         else:
@@ -117,8 +117,10 @@ class Server:
 
     def __init__(self, backend, budget_bytes: int, chunk: int = 25, max_active: int = 256,
                  clock: Callable[[], float] = time.monotonic, sleep: Callable[[float], None] = time.sleep,
-                 idle_sleep: float = 2e-4):
+                 idle_sleep: float = 2e-4, prioritize: bool = True, levels: int = 6):
         self.backend = backend
+        self.prioritize = prioritize
+        self.levels = levels
         self.budget = int(budget_bytes)
         self.chunk = int(chunk)
         self.max_active = int(max_active)
@@ -128,6 +130,17 @@ class Server:
         self.used = 0
         self.peak_used = 0
         self._cancel = set()
+
+    def _priority(self, req: SolveRequest, nbytes: int) -> int:
+        """Stream priority by expected work (steps x bytes): shorter runs get
+        precedence on the device (lower value = higher priority), so small
+        requests are not held behind large ones that share the GPU."""
+        if not self.prioritize:
+            return 0
+        work = max(1.0, float(req.nsteps) * float(nbytes))
+        # one level per factor 2^2.5 of work above 2^30 byte-steps; the largest runs get 0 (lowest)
+        level = max(0, min(self.levels - 1, int((np.log2(work) - 30.0) / 2.5)))
+        return -(self.levels - 1 - level)
 
     def cancel(self, rid: int):
         """Stops a queued or running request at its next chunk boundary."""
@@ -188,7 +201,7 @@ class Server:
                 self.used += nb
                 self.peak_used = max(self.peak_used, self.used)
                 try:
-                    inst = self.backend.create(req)
+                    inst = self.backend.create(req, self._priority(req, nb))
                 except Exception as exc:
                     self.used -= nb
                     results[req.rid].status, results[req.rid].error = "failed", str(exc)

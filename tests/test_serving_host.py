@@ -35,7 +35,7 @@ class SimBackend:
             raise ValueError("invalid sizes or length factors")
         return req.args.Nx ** 3 * self.bytes_per_mode
 
-    def create(self, req):
+    def create(self, req, priority=0):
         if req.rid in self.fail_create:
             raise RuntimeError("device allocation failed")
         inst = {"req": req, "done_at": 0.0, "steps": 0, "pending": 0}
@@ -161,3 +161,13 @@ def test_synthetic_workload_matches_the_served_mix():
     gaps = np.diff([0.0] + [r.arrival for r in reqs])
     assert abs(gaps.mean() - 1 / 20.0) < 0.01
     assert any(r.args.isLES for r in reqs) and any(not r.args.isLES for r in reqs)
+
+
+def test_shorter_runs_get_higher_stream_priority():
+    clock = FakeClock()
+    srv = _server(SimBackend(clock), clock, budget=10 ** 12)
+    small = SolveRequest(0, box_args(32, nu=1e-2), 200)
+    big = SolveRequest(1, box_args(256, nu=1e-2), 2000)
+    p_small = srv._priority(small, 32 ** 3 * 1000)
+    p_big = srv._priority(big, 256 ** 3 * 1000)
+    assert p_small < p_big <= 0
