@@ -21,29 +21,42 @@
 
 namespace spns {
 
-// Plane group geometry: 2-D arrays [r][c] (c contiguous) of R x C complex.
-struct EdgePlanes {
-    int axis;        // 0 x, 1 y, 2 z
-    int nplanes;     // 2 for x, y; 1 for z
+// A set of axes whose plane groups share the 2-D transform size R x C (all
+// three for a cubic box), corrected together so that each phase is one launch.
+// Planes are numbered over the set: axis slot k owns planes first[k] ..
+// first[k+1]-1 (2 for x and y, s = +1 then -1; 1 for z).  Buffers:
+//   V   [plane][comp][R][C]   source-plane velocities, then their 2-D inverse DFT
+//   Phi [plane][R][C]         phi = 1/2 sum_j V_j^2, then its 2-D forward DFT
+struct EdgeSet {
+    int naxes;
+    int axis[3];     // 0 x, 1 y, 2 z
+    int first[4];
     int R, C;        // FFT grid of the two other axes (rows strided, columns contiguous)
 };
 
+__device__ __forceinline__ int edge_slot(const EdgeSet &es, int plane) {
+    int k = 0;
+    while (k + 1 < es.naxes && plane >= es.first[k + 1]) k++;
+    return k;
+}
+
 // Source-plane coefficients of the three velocity components, zero padded to
-// the R x C grid.  out: [plane][comp][R][C].
+// the R x C grid.
 template <typename T>
-__global__ void k_edge_build(Geo g, const cx<T> *__restrict__ U, EdgePlanes ep, cx<T> *__restrict__ out) {
-    const long long n = (long long)ep.R * ep.C;
-    const long long tot = n * 3 * ep.nplanes;
+__global__ void k_edge_build(Geo g, const cx<T> *__restrict__ U, EdgeSet es, cx<T> *__restrict__ out) {
+    const long long n = (long long)es.R * es.C;
+    const long long tot = n * 3 * es.first[es.naxes];
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
         const long long rc = t % n;
-        const int comp = (int)((t / n) % 3), pl = (int)(t / (n * 3));
-        const int r = (int)(rc / ep.C), c = (int)(rc % ep.C);
-        const int s = ep.axis == 2 ? 1 : (pl == 0 ? 1 : -1);  // destination sign
-        const int pr = ffreq(r, ep.R), pc = ffreq(c, ep.C);
+        const int comp = (int)((t / n) % 3), plane = (int)(t / (n * 3));
+        const int k = edge_slot(es, plane), axis = es.axis[k], pl = plane - es.first[k];
+        const int r = (int)(rc / es.C), c = (int)(rc % es.C);
+        const int s = axis == 2 ? 1 : (pl == 0 ? 1 : -1);  // destination sign
+        const int pr = ffreq(r, es.R), pc = ffreq(c, es.C);
         // source mode (px, py, pz) on plane p_axis = -s*h
         int px, py, pz;
-        if (ep.axis == 0) { px = -s * g.hx; py = pr; pz = pc; }
-        else if (ep.axis == 1) { px = pr; py = -s * g.hy; pz = pc; }
+        if (axis == 0) { px = -s * g.hx; py = pr; pz = pc; }
+        else if (axis == 1) { px = pr; py = -s * g.hy; pz = pc; }
         else { px = pr; py = pc; pz = -g.hz; }
         cx<T> val = zero<T>();
         if (px >= -g.hx && px <= g.hx && py >= -g.hy && py <= g.hy && pz >= -g.hz && pz <= g.hz) {
@@ -70,38 +83,42 @@ __global__ void k_edge_square(const cx<T> *__restrict__ V, long long n, int npla
     }
 }
 
-// G_axis(k) += i (-s L M) M Phi(k_perp) on the kept modes of the destination planes.
+// G_axis(k) += i (-s L M) M Phi(k_perp) on the kept modes of the destination
+// planes.  blockIdx.y = axis slot of the set.
 template <typename T>
-__global__ void k_edge_apply(Geo g, cx<T> *__restrict__ G, EdgePlanes ep, const cx<T> *__restrict__ Phi) {
-    const long long n = (long long)ep.R * ep.C;
+__global__ void k_edge_apply(Geo g, cx<T> *__restrict__ G, EdgeSet es, const cx<T> *__restrict__ Phi) {
+    const int k = blockIdx.y;
+    if (k >= es.naxes) return;
+    const int axis = es.axis[k], nplanes = es.first[k + 1] - es.first[k];
+    const long long n = (long long)es.R * es.C;
     int A, B;  // kept extents of the two other axes: (ky, kz), (kx, kz), (kx, ky)
-    if (ep.axis == 0) { A = g.Ky; B = g.Kz; } else if (ep.axis == 1) { A = g.Kx; B = g.Kz; } else { A = g.Kx; B = g.Ky; }
-    const long long tot = (long long)A * B * ep.nplanes;
-    const double M = ep.axis == 0 ? g.Mx : ep.axis == 1 ? g.My : g.Mz;
-    const double Ls = ep.axis == 0 ? g.sx : ep.axis == 1 ? g.sy : g.sz;
+    if (axis == 0) { A = g.Ky; B = g.Kz; } else if (axis == 1) { A = g.Kx; B = g.Kz; } else { A = g.Kx; B = g.Ky; }
+    const long long tot = (long long)A * B * nplanes;
+    const double M = axis == 0 ? g.Mx : axis == 1 ? g.My : g.Mz;
+    const double Ls = axis == 0 ? g.sx : axis == 1 ? g.sy : g.sz;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
         const int pl = (int)(t / ((long long)A * B));
         const int ab = (int)(t % ((long long)A * B));
         const int ia = ab / B, ib = ab % B;
-        const int s = ep.axis == 2 ? 1 : (pl == 0 ? 1 : -1);
+        const int s = axis == 2 ? 1 : (pl == 0 ? 1 : -1);
         int ix, iy, kz, r, c;
-        if (ep.axis == 0) {
+        if (axis == 0) {
             const int my = ia <= g.hy ? ia : ia - g.Ky;
             ix = s > 0 ? g.hx : g.Kx - g.hx; iy = ia; kz = ib;
-            r = my >= 0 ? my : my + ep.R; c = kz;
-        } else if (ep.axis == 1) {
+            r = my >= 0 ? my : my + es.R; c = kz;
+        } else if (axis == 1) {
             const int mx = ia <= g.hx ? ia : ia - g.Kx;
             ix = ia; iy = s > 0 ? g.hy : g.Ky - g.hy; kz = ib;
-            r = mx >= 0 ? mx : mx + ep.R; c = kz;
+            r = mx >= 0 ? mx : mx + es.R; c = kz;
         } else {
             const int mx = ia <= g.hx ? ia : ia - g.Kx, my = ib <= g.hy ? ib : ib - g.Ky;
             ix = ia; iy = ib; kz = g.hz;
-            r = mx >= 0 ? mx : mx + ep.R; c = my >= 0 ? my : my + ep.C;
+            r = mx >= 0 ? mx : mx + es.R; c = my >= 0 ? my : my + es.C;
         }
-        const cx<T> ph = Phi[pl * n + (long long)r * ep.C + c];
+        const cx<T> ph = Phi[(long long)(es.first[k] + pl) * n + (long long)r * es.C + c];
         const T f = T(-(double)s * Ls * M * M);  // i * f * Phi
         const long long idx = ((long long)iy * g.Kx + ix) * g.Kz + kz;
-        cx<T> *dst = G + (long long)ep.axis * g.S0 + idx;
+        cx<T> *dst = G + (long long)axis * g.S0 + idx;
         *dst = *dst + mul_i(f * ph);
     }
 }

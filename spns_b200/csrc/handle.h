@@ -94,7 +94,7 @@ template <typename T, int L, int MODE> struct Shape3 {
     static constexpr int Q = L / E;
     static constexpr int ZT = ShapeSel<T>::Z_T / Q;
     static constexpr int P0 = ZT >= 32 ? 32 : ZT >= 16 ? 16 : ZT >= 8 ? 8 : ZT >= 4 ? 4 : ZT >= 2 ? 2 : 1;
-    static constexpr size_t PER_PEN = (size_t)spns::SmPencil<T, L>::PITCH * sizeof(spns::cx<T>) + (size_t)spns::K3Phys<MODE>::N * L * sizeof(T);
+    static constexpr size_t PER_PEN = (size_t)spns::SmPencil<T, L>::PITCH * sizeof(spns::cx<T>) + (size_t)spns::K3Reg<T, MODE>::NSM * L * sizeof(T);
     static constexpr int PMAX = (int)((200 * 1024) / PER_PEN);
     static constexpr int P = P0 <= PMAX ? P0 : PMAX >= 16 ? 16 : PMAX >= 8 ? 8 : PMAX >= 4 ? 4 : PMAX >= 2 ? 2 : 1;
     static constexpr int THREADS = P * Q;
@@ -131,6 +131,7 @@ struct spns_handle {
     std::map<int, void *> tw;                        // twiddle tables per length (precision of the handle)
     std::string err;
     int kernels_per_step = 0;
+    int edge_launches = 0;                           // launches of the edge correction in the last step
     // CUDA graphs of one step, per parity of the state-buffer swap (kappa scheme)
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     void *U0 = nullptr;                              // state buffer of parity 0
@@ -200,8 +201,10 @@ template <typename T> inline void *spns_make_twiddles(int L, cudaStream_t st) {
     return d;
 }
 
+// Opt-in to the dynamic shared memory of a launch.  Set even below 48 KB: the
+// kernel's static shared memory counts against the same 48 KB default limit.
 template <class K> inline cudaError_t spns_set_smem(K kern, size_t bytes) {
-    if (bytes <= 48 * 1024) return cudaSuccess;
+    if (bytes <= 16 * 1024) return cudaSuccess;
     return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 

@@ -151,27 +151,40 @@ template <typename T> struct Passes {
     // (edge_kernels.cuh), added to the compact nonlinear term G held in B2.
     static int edge_correction(spns_handle *h) {
         const spns::Geo &g = h->g;
-        for (int axis = 0; axis < 3; axis++) {
-            if (!h->edge_axis[axis]) continue;
-            spns::EdgePlanes ep;
-            ep.axis = axis;
-            ep.nplanes = axis == 2 ? 1 : 2;
-            ep.R = axis == 0 ? g.My : g.Mx;
-            ep.C = axis == 2 ? g.My : g.Mz;
-            const long long n = (long long)ep.R * ep.C;
-            C *V = (C *)h->edge, *Phi = V + 3 * 2 * n;
-            const long long nb = n * 3 * ep.nplanes;
+        // group the aliasing axes by the size of their 2-D transforms (one group for a cubic box)
+        int RC[3][2] = {{g.My, g.Mz}, {g.Mx, g.Mz}, {g.Mx, g.My}};
+        bool done[3] = {false, false, false};
+        for (int a0 = 0; a0 < 3; a0++) {
+            if (!h->edge_axis[a0] || done[a0]) continue;
+            spns::EdgeSet es;
+            es.naxes = 0;
+            es.R = RC[a0][0];
+            es.C = RC[a0][1];
+            es.first[0] = 0;
+            for (int a = a0; a < 3; a++) {
+                if (!h->edge_axis[a] || done[a] || RC[a][0] != es.R || RC[a][1] != es.C) continue;
+                done[a] = true;
+                es.axis[es.naxes] = a;
+                es.first[es.naxes + 1] = es.first[es.naxes] + (a == 2 ? 1 : 2);
+                es.naxes++;
+            }
+            const int np = es.first[es.naxes];
+            const long long n = (long long)es.R * es.C;
+            C *V = (C *)h->edge, *Phi = V + 3 * (long long)np * n;
+            const long long nb = n * 3 * np;
             const int blocks = (int)std::min<long long>((nb + 255) / 256, 148 * 16);
-            spns::k_edge_build<T><<<blocks, 256, 0, h->st>>>(g, U(h), ep, V);
+            spns::k_edge_build<T><<<blocks, 256, 0, h->st>>>(g, U(h), es, V);
             CKL();
-            DISPATCH(ep.C, LAUNCH((launch_lines<LL, true>(h, V, (long long)ep.R * 3 * ep.nplanes))));
-            DISPATCH(ep.R, LAUNCH((launch_cols<LL, true>(h, V, ep.C, 3 * ep.nplanes))));
-            spns::k_edge_square<T><<<blocks, 256, 0, h->st>>>(V, n, ep.nplanes, Phi);
+            DISPATCH(es.C, LAUNCH((launch_lines<LL, true>(h, V, (long long)es.R * 3 * np))));
+            DISPATCH(es.R, LAUNCH((launch_cols<LL, true>(h, V, es.C, 3 * np))));
+            spns::k_edge_square<T><<<blocks, 256, 0, h->st>>>(V, n, np, Phi);
             CKL();
-            DISPATCH(ep.C, LAUNCH((launch_lines<LL, false>(h, Phi, (long long)ep.R * ep.nplanes))));
-            DISPATCH(ep.R, LAUNCH((launch_cols<LL, false>(h, Phi, ep.C, ep.nplanes))));
-            spns::k_edge_apply<T><<<blocks, 256, 0, h->st>>>(g, (C *)h->B2, ep, Phi);
+            DISPATCH(es.C, LAUNCH((launch_lines<LL, false>(h, Phi, (long long)es.R * np))));
+            DISPATCH(es.R, LAUNCH((launch_cols<LL, false>(h, Phi, es.C, np))));
+            const int ablocks = (int)std::min<long long>((n * 2 + 255) / 256, 148 * 8);
+            spns::k_edge_apply<T><<<dim3(ablocks, es.naxes), 256, 0, h->st>>>(g, (C *)h->B2, es, Phi);
             CKL();
+            h->edge_launches += 7;
         }
         return SPNS_OK;
     }
@@ -187,6 +200,7 @@ template <typename T> struct Passes {
     // One New_Fractional_Step_Method (src/HIT_LES.cpp:9-25).
     static int step_once(spns_handle *h) {
         int nk = 0;
+        h->edge_launches = 0;
         int slot = 0;
         const bool prof = h->prof_steps < h->prof_cap_steps;
 #define MARK(name) do { if (prof) prof_mark(h, slot++, name); } while (0)
@@ -230,8 +244,7 @@ template <typename T> struct Passes {
         CKL();
         MARK(nullptr);
         if (prof) { if (h->prof_steps == 0) h->prof_nk = slot - 1; h->prof_steps++; }
-        if (mode == spns::MODE_ROT && h->edge)
-            for (int axis = 0; axis < 3; axis++) nk += h->edge_axis[axis] ? 7 : 0;   // build, 2+2 line FFTs, square, apply
+        if (mode == spns::MODE_ROT && h->edge) nk += h->edge_launches;             // build, 2+2 line FFTs, square, apply per group
         h->kernels_per_step = nk + 8;
         return SPNS_OK;
 #undef MARK

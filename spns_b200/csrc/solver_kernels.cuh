@@ -287,6 +287,40 @@ __device__ __forceinline__ void k3_store_single(cx<T> (&r)[E], SmPencil<T, L> sm
     }
 }
 
+// One forward job of the z pass: a pair (k3_store_pair) or, with `single`, a
+// single real field (k3_store_single), behind one copy of the transform code.
+template <typename T, int L, int E>
+__device__ __forceinline__ void k3_store_job(cx<T> (&r)[E], SmPencil<T, L> sm, int q, int Kz, cx<T> *A, cx<T> *B, bool fold,
+                                             bool single, T sz, bool ok, const cx<T> *__restrict__ tw) {
+    constexpr int Q = L / E;
+    fft<T, L, E, false, SmPencil<T, L>, (32 % (L / E) == 0)>(r, sm, q, tw);
+    if (single) {
+        if (ok) {
+#pragma unroll
+            for (int e = 0; e < E; e++) {
+                const int row = out_row<L, E, false>(q, e);
+                if (row < Kz) A[row] = r[e];
+            }
+        }
+        return;
+    }
+#pragma unroll
+    for (int e = 0; e < E; e++) sm.at(out_row<L, E, false>(q, e)) = r[e];
+    __syncthreads();
+    if (ok) {
+        const T h = T(0.5);
+        for (int k = q; k < Kz; k += Q) {
+            cx<T> zk = sm.at(k), zm = sm.at(k == 0 ? 0 : L - k);
+            cx<T> xa = mk<T>(h * (zk.x + zm.x), h * (zk.y - zm.y));
+            cx<T> xb = mk<T>(h * (zk.y + zm.y), h * (zm.x - zk.x));
+            if (fold) xa = xa + mul_i(T(k) * sz * xb);
+            A[k] = xa;
+            if (B) B[k] = xb;
+        }
+    }
+    __syncthreads();
+}
+
 // Running CFL maxima; a NaN or Inf velocity turns the maxima into +Inf (fmax
 // alone would drop NaN), which the block reduction reports as non-finite.
 template <typename T>
@@ -311,6 +345,25 @@ template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile(
 // Shared-memory slots of physical fields kept per pencil (rows of this thread only).
 // slots: 0 u, 1 v, 2 w, 3..5 conv_x,y,z, LES 6..11 a11, a12, a22, a13, a23, a33 (then t_ij)
 template <int MODE> struct K3Phys { static constexpr int N = MODE == MODE_ADV ? 6 : MODE == MODE_LES ? 12 : 0; };
+// The first slots live in registers (indexed by the thread's register slot e, not
+// by row), the rest in shared memory: the twelve LES slots of a 384-pencil take
+// 37 KB of shared memory in FP64, which alone would allow 4 pencils per SM.
+#ifndef SPNS_K3_REG_SLOTS
+#define SPNS_K3_REG_SLOTS 6
+#endif
+#ifndef SPNS_F32_K3_REG_SLOTS
+#define SPNS_F32_K3_REG_SLOTS 9
+#endif
+template <typename T, int MODE> struct K3Reg {
+    static constexpr int R = sizeof(T) == 8 ? SPNS_K3_REG_SLOTS : SPNS_F32_K3_REG_SLOTS;
+    static constexpr int N = K3Phys<MODE>::N < R ? K3Phys<MODE>::N : R;   // slots in registers
+    static constexpr int NSM = K3Phys<MODE>::N - N;                       // slots in shared memory
+};
+template <int S, int NREG, int L, typename T, int E>
+__device__ __forceinline__ T &k3_slot(T (&rg)[NREG > 0 ? NREG : 1][E], T *ph, int e, int row) {
+    if constexpr (S < NREG) return rg[S][e];
+    else return ph[(S - NREG) * L + row];
+}
 
 // STAGE (rotational form): the six input fields of the block's pencils are
 // copied into shared memory asynchronously at the start, in the order the
@@ -322,7 +375,6 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
                                                    double *__restrict__ phys, const cx<T> *__restrict__ tw) {
     extern __shared__ __align__(16) unsigned char smraw[];
     constexpr int Q = L / E;
-    constexpr int NPH = K3Phys<MODE>::N;
     const int tid = threadIdx.x, p = tid / Q, q = tid % Q;
     const long long npen = (long long)g.Mx * g.My;
     const long long pen = (long long)blockIdx.x * P + p;
@@ -330,7 +382,8 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
     const long long base = (ok ? pen : 0) * g.Kz;
     cx<T> *smc = reinterpret_cast<cx<T> *>(smraw);
     SmPencil<T, L> sm{smc + p * SmPencil<T, L>::PITCH};
-    T *ph = reinterpret_cast<T *>(smc + P * SmPencil<T, L>::PITCH) + (long long)p * NPH * L;
+    constexpr int NREG = K3Reg<T, MODE>::N;
+    T *ph = reinterpret_cast<T *>(smc + P * SmPencil<T, L>::PITCH) + (long long)p * K3Reg<T, MODE>::NSM * L;
     const T sz = T(g.sz);
     cx<T> *const B0 = buf + base;
 #define F(i) (B0 + (long long)(i) * g.S2)
@@ -406,75 +459,77 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
         // Advective form of the reference (src/HIT_LES.cpp:74-125): conv_i = u_j d_j u_i.
         // S2 inputs: 0 u, 1 v, 2 w, 3 du/dx, 4 dv/dx, 5 dw/dx, 6 du/dy, 7 dv/dy, 8 dw/dy;
         // z-derivatives are formed here from u, v, w.  Physical values of the
-        // thread's own rows are kept in per-thread shared-memory slots (no barrier needed).
+        // thread's own rows are kept in per-thread slots, the first K3Reg::N in
+        // registers and the rest in shared memory (own rows only: no barrier needed).
         // LES (src/HIT_LES.cpp:130-171): strain combinations a_ij accumulate in further slots.
+        // The transforms run in two loops (inverse pairs, forward jobs) around one
+        // copy of the transform code each: unrolled one after another, the eleven
+        // LES transforms overflow the instruction cache.
         cx<T> A[E];
-#define PH(slot, row) ph[(slot) * L + (row)]
-        // (u, v)
-        k3_load_pair<T, L, E>(A, F(0), false, F(1), false, g.Kz, sz, q, ok);
-        fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(A, sm, q, tw);
+        T rg[NREG > 0 ? NREG : 1][E];
+#define PH(slot, row) k3_slot<(slot), NREG, L, T, E>(rg, ph, e, row)
+        // inverse pairs: (u, v), (w, du/dz), (du/dx, du/dy), (dv/dx, dv/dy), (dw/dx, dw/dy), (dv/dz, dw/dz)
+#pragma unroll 1
+        for (int pi = 0; pi < 6; pi++) {
+            const int fa = pi == 0 ? 0 : pi == 1 ? 2 : pi == 5 ? 1 : pi + 1;
+            const int fb = pi == 0 ? 1 : pi == 1 ? 0 : pi == 5 ? 2 : pi + 4;
+            k3_load_pair<T, L, E>(A, F(fa), pi == 5, F(fb), pi == 1 || pi == 5, g.Kz, sz, q, ok);
+            fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(A, sm, q, tw);
+            switch (pi) {
+            case 0:
 #pragma unroll
-        for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); PH(0, row) = A[e].x; PH(1, row) = A[e].y; }
-        // (w, du/dz)
-        k3_load_pair<T, L, E>(A, F(2), false, F(0), true, g.Kz, sz, q, ok);
-        fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(A, sm, q, tw);
+                for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); PH(0, row) = A[e].x; PH(1, row) = A[e].y; }
+                break;
+            case 1:
 #pragma unroll
-        for (int e = 0; e < E; e++) {
-            const int row = out_row<L, E, true>(q, e);
-            const T ww = A[e].x;
-            PH(2, row) = ww;
-            cfl_update<T>(mx, PH(0, row), PH(1, row), ww, c);
-            PH(3, row) = ww * A[e].y;
-            if (MODE == MODE_LES) PH(9, row) = A[e].y; // a13 = du/dz (+ dw/dx below)
-        }
-        // (du/dx, du/dy)
-        k3_load_pair<T, L, E>(A, F(3), false, F(6), false, g.Kz, sz, q, ok);
-        fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(A, sm, q, tw);
+                for (int e = 0; e < E; e++) {
+                    const int row = out_row<L, E, true>(q, e);
+                    const T ww = A[e].x;
+                    PH(2, row) = ww;
+                    cfl_update<T>(mx, PH(0, row), PH(1, row), ww, c);
+                    PH(3, row) = ww * A[e].y;
+                    if (MODE == MODE_LES) PH(9, row) = A[e].y; // a13 = du/dz (+ dw/dx below)
+                }
+                break;
+            case 2:
 #pragma unroll
-        for (int e = 0; e < E; e++) {
-            const int row = out_row<L, E, true>(q, e);
-            PH(3, row) = PH(0, row) * A[e].x + PH(1, row) * A[e].y + PH(3, row);
-            if (MODE == MODE_LES) { PH(6, row) = A[e].x; PH(7, row) = A[e].y; } // a11, a12 (partial)
-        }
-        // (dv/dx, dv/dy)
-        k3_load_pair<T, L, E>(A, F(4), false, F(7), false, g.Kz, sz, q, ok);
-        fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(A, sm, q, tw);
+                for (int e = 0; e < E; e++) {
+                    const int row = out_row<L, E, true>(q, e);
+                    PH(3, row) = PH(0, row) * A[e].x + PH(1, row) * A[e].y + PH(3, row);
+                    if (MODE == MODE_LES) { PH(6, row) = A[e].x; PH(7, row) = A[e].y; } // a11, a12 (partial)
+                }
+                break;
+            case 3:
 #pragma unroll
-        for (int e = 0; e < E; e++) {
-            const int row = out_row<L, E, true>(q, e);
-            PH(4, row) = PH(0, row) * A[e].x + PH(1, row) * A[e].y;
-            if (MODE == MODE_LES) { PH(7, row) = PH(7, row) + A[e].x; PH(8, row) = A[e].y; } // a12, a22
-        }
-        // (dw/dx, dw/dy)
-        k3_load_pair<T, L, E>(A, F(5), false, F(8), false, g.Kz, sz, q, ok);
-        fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(A, sm, q, tw);
+                for (int e = 0; e < E; e++) {
+                    const int row = out_row<L, E, true>(q, e);
+                    PH(4, row) = PH(0, row) * A[e].x + PH(1, row) * A[e].y;
+                    if (MODE == MODE_LES) { PH(7, row) = PH(7, row) + A[e].x; PH(8, row) = A[e].y; } // a12, a22
+                }
+                break;
+            case 4:
 #pragma unroll
-        for (int e = 0; e < E; e++) {
-            const int row = out_row<L, E, true>(q, e);
-            PH(5, row) = PH(0, row) * A[e].x + PH(1, row) * A[e].y;
-            if (MODE == MODE_LES) { PH(9, row) = PH(9, row) + A[e].x; PH(10, row) = A[e].y; } // a13, a23 (partial)
-        }
-        // (dv/dz, dw/dz)
-        k3_load_pair<T, L, E>(A, F(1), true, F(2), true, g.Kz, sz, q, ok);
-        fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(A, sm, q, tw);
+                for (int e = 0; e < E; e++) {
+                    const int row = out_row<L, E, true>(q, e);
+                    PH(5, row) = PH(0, row) * A[e].x + PH(1, row) * A[e].y;
+                    if (MODE == MODE_LES) { PH(9, row) = PH(9, row) + A[e].x; PH(10, row) = A[e].y; } // a13, a23 (partial)
+                }
+                break;
+            default:
 #pragma unroll
-        for (int e = 0; e < E; e++) {
-            const int row = out_row<L, E, true>(q, e);
-            const T ww = PH(2, row);
-            PH(4, row) = PH(4, row) + ww * A[e].x;
-            PH(5, row) = PH(5, row) + ww * A[e].y;
-            if (MODE == MODE_LES) { PH(10, row) = PH(10, row) + A[e].x; PH(11, row) = A[e].y; } // a23, a33
+                for (int e = 0; e < E; e++) {
+                    const int row = out_row<L, E, true>(q, e);
+                    const T ww = PH(2, row);
+                    PH(4, row) = PH(4, row) + ww * A[e].x;
+                    PH(5, row) = PH(5, row) + ww * A[e].y;
+                    if (MODE == MODE_LES) { PH(10, row) = PH(10, row) + A[e].x; PH(11, row) = A[e].y; } // a23, a33
+                }
+                break;
+            }
         }
         if (!ok) { mx[0] = mx[1] = mx[2] = mx[3] = 0.0; }
         block_max4<T>(mx, ds);
-        if constexpr (MODE == MODE_ADV) {
-#pragma unroll
-            for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(PH(3, row), PH(4, row)); }
-            k3_store_pair<T, L, E>(A, sm, q, g.Kz, F(0), F(1), false, sz, ok, tw);
-#pragma unroll
-            for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(PH(5, row), T(0)); }
-            k3_store_single<T, L, E>(A, sm, q, g.Kz, F(2), ok, tw);
-        } else {
+        if constexpr (MODE == MODE_LES) {
             // eddy viscosity and SGS stress (src/HIT_LES.cpp:130-154), written over the a_ij slots:
             // slot 6 t11, 7 t12, 8 t22, 9 t13, 10 t23, 11 t33
             const T ct = T(c.les_ct);
@@ -496,22 +551,54 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
                 PH(10, row) = T(-1.0) * ne * a23;
                 PH(11, row) = T(-2.0) * ne * a33;
             }
-            // outputs: 0 G_x = conv_x + i kz t13, 1 G_y, 2 G_z, 3 t11, 4 t12, 5 t13, 6 t22, 7 t23
+        }
+        // forward jobs.  ADV: (conv_x, conv_y) -> 0, 1; conv_z -> 2.
+        // LES outputs: 0 G_x = conv_x + i kz t13, 1 G_y, 2 G_z, 3 t11, 4 t12, 5 t13, 6 t22, 7 t23
+        constexpr int NJOB = MODE == MODE_LES ? 5 : 2;
+#pragma unroll 1
+        for (int j = 0; j < NJOB; j++) {
+            cx<T> *oa, *ob = nullptr;
+            bool fold = false, single = false;
+            if (MODE == MODE_ADV) {
+                if (j == 0) {
 #pragma unroll
-            for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(PH(3, row), PH(9, row)); }
-            k3_store_pair<T, L, E>(A, sm, q, g.Kz, F(0), F(5), true, sz, ok, tw);
+                    for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(PH(3, row), PH(4, row)); }
+                    oa = F(0); ob = F(1);
+                } else {
 #pragma unroll
-            for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(PH(4, row), PH(10, row)); }
-            k3_store_pair<T, L, E>(A, sm, q, g.Kz, F(1), F(7), true, sz, ok, tw);
+                    for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(PH(5, row), T(0)); }
+                    oa = F(2); single = true;
+                }
+            } else {
+                switch (j) {
+                case 0:
 #pragma unroll
-            for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(PH(5, row), PH(11, row)); }
-            k3_store_pair<T, L, E>(A, sm, q, g.Kz, F(2), nullptr, true, sz, ok, tw);
+                    for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(PH(3, row), PH(9, row)); }
+                    oa = F(0); ob = F(5); fold = true;
+                    break;
+                case 1:
 #pragma unroll
-            for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(PH(6, row), PH(7, row)); }
-            k3_store_pair<T, L, E>(A, sm, q, g.Kz, F(3), F(4), false, sz, ok, tw);
+                    for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(PH(4, row), PH(10, row)); }
+                    oa = F(1); ob = F(7); fold = true;
+                    break;
+                case 2:
 #pragma unroll
-            for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(PH(8, row), T(0)); }
-            k3_store_single<T, L, E>(A, sm, q, g.Kz, F(6), ok, tw);
+                    for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(PH(5, row), PH(11, row)); }
+                    oa = F(2); fold = true;
+                    break;
+                case 3:
+#pragma unroll
+                    for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(PH(6, row), PH(7, row)); }
+                    oa = F(3); ob = F(4);
+                    break;
+                default:
+#pragma unroll
+                    for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(PH(8, row), T(0)); }
+                    oa = F(6); single = true;
+                    break;
+                }
+            }
+            k3_store_job<T, L, E>(A, sm, q, g.Kz, oa, ob, fold, single, sz, ok, tw);
         }
 #undef PH
     }

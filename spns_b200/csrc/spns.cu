@@ -310,7 +310,8 @@ static BufferPlan buffer_plan(const spns_hit_args &a, const Geo &g, int last_rad
     p.B1 = cs * p.nB1 * (size_t)g.S1;
     p.B2 = cs * p.nB2 * (size_t)g.S2;
     p.bins = sizeof(double) * 2 * (size_t)(last_rad_max + 1);
-    p.edge = p.need_edge ? cs * 8 * (size_t)std::max((long long)g.My * g.Mz, std::max((long long)g.Mx * g.Mz, (long long)g.Mx * g.My)) : 0;
+    // up to 5 planes of one axis set: 3 components each for V plus one Phi plane each
+    p.edge = p.need_edge ? cs * 20 * (size_t)std::max((long long)g.My * g.Mz, std::max((long long)g.Mx * g.Mz, (long long)g.Mx * g.My)) : 0;
     p.tw = cs * ((size_t)g.Mx + g.My + g.Mz);
     p.scalars = sizeof(DevScalars);
     return p;
