@@ -60,7 +60,7 @@ template <typename T, int L, int E_, int THR> struct ShapeT {
 #define SPNS_F32_Z_E 12
 #endif
 #ifndef SPNS_F32_Z_T
-#define SPNS_F32_Z_T 256
+#define SPNS_F32_Z_T 128
 #endif
 #ifndef SPNS_Z_THREADS
 #define SPNS_Z_THREADS 128    // threads per block in the double z pass (2 blocks per SM)
@@ -74,6 +74,12 @@ template <typename T, int L, int E_, int THR> struct ShapeT {
 #ifndef SPNS_F32_Z_STAGE
 #define SPNS_F32_Z_STAGE 1
 #endif
+#ifndef SPNS_Z_E_ROT
+#define SPNS_Z_E_ROT SPNS_Z_E
+#endif
+#ifndef SPNS_F32_Z_E_ROT
+#define SPNS_F32_Z_E_ROT 12
+#endif
 template <typename T> struct ShapeSel {
     static constexpr bool D = sizeof(T) == 8;
     static constexpr int K1_E = D ? 12 : SPNS_F32_K1_E, K1_T = D ? 256 : SPNS_F32_K1_T;
@@ -81,6 +87,7 @@ template <typename T> struct ShapeSel {
     static constexpr int K5_E = D ? 24 : SPNS_F32_K5_E, K5_T = D ? 128 : SPNS_F32_K5_T;
     static constexpr int Z_E = D ? SPNS_Z_E : SPNS_F32_Z_E, Z_T = D ? SPNS_Z_THREADS : SPNS_F32_Z_T;
     static constexpr bool Z_STAGE = D ? SPNS_Z_STAGE : SPNS_F32_Z_STAGE;
+    static constexpr int Z_E_ROT = D ? SPNS_Z_E_ROT : SPNS_F32_Z_E_ROT;   // rotational/velocity z pass
 };
 template <typename T, int L> using ShapeK1 = ShapeT<T, L, ShapeSel<T>::K1_E, ShapeSel<T>::K1_T>;   // inverse x
 template <typename T, int L> using ShapeK2 = ShapeT<T, L, ShapeSel<T>::K2_E, ShapeSel<T>::K2_T>;   // inverse y (and forward y)
@@ -90,7 +97,7 @@ template <typename T, int L> using Shape = ShapeT<T, L, 24, 128>;               
 // z pass: pencils per block limited by the shared memory of the exchange
 // buffer plus the physical fields kept per pencil.
 template <typename T, int L, int MODE> struct Shape3 {
-    static constexpr int E = ShapeSel<T>::Z_E;   // the z pass keeps several fields in registers
+    static constexpr int E = (MODE == spns::MODE_ROT || MODE == spns::MODE_VEL) ? ShapeSel<T>::Z_E_ROT : ShapeSel<T>::Z_E;
     static constexpr int Q = L / E;
     static constexpr int ZT = ShapeSel<T>::Z_T / Q;
     static constexpr int P0 = ZT >= 32 ? 32 : ZT >= 16 ? 16 : ZT >= 8 ? 8 : ZT >= 4 ? 4 : ZT >= 2 ? 2 : 1;

@@ -354,6 +354,12 @@ template <int MODE> struct K3Phys { static constexpr int N = MODE == MODE_ADV ? 
 #ifndef SPNS_F32_K3_REG_SLOTS
 #define SPNS_F32_K3_REG_SLOTS 9
 #endif
+#ifndef SPNS_K3_ROT_LOOP
+#define SPNS_K3_ROT_LOOP 1    // double rotational z pass: one copy of the forward transform code
+#endif
+#ifndef SPNS_F32_K3_ROT_LOOP
+#define SPNS_F32_K3_ROT_LOOP 1
+#endif
 template <typename T, int MODE> struct K3Reg {
     static constexpr int R = sizeof(T) == 8 ? SPNS_K3_REG_SLOTS : SPNS_F32_K3_REG_SLOTS;
     static constexpr int N = K3Phys<MODE>::N < R ? K3Phys<MODE>::N : R;   // slots in registers
@@ -436,6 +442,54 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
             cp_async_wait<2>();
             __syncthreads();
         }
+        constexpr bool ROT_LOOP = sizeof(T) == 8 ? SPNS_K3_ROT_LOOP : SPNS_F32_K3_ROT_LOOP;
+        if constexpr (ROT_LOOP) {
+        // one copy of the transform code: the pairs in a loop, physical values in register slots
+        // 0 u, 1 w_x, 2 v, 3 w_y, 4 c_z
+        (void)B; (void)C;
+        // The pair loop is unrolled (three transform copies; the two forward jobs share
+        // one): rolled, with slots written in one iteration and read in a later
+        // one, it computed wrong products.  The slots are defined on entry all the same.
+        T rs[5][E];
+#pragma unroll
+        for (int i = 0; i < 5; i++)
+#pragma unroll
+            for (int e = 0; e < E; e++) rs[i][e] = T(0);
+        const cx<T> *sbase = src[0];
+        const long long sstride = src[1] - src[0];
+#pragma unroll
+        for (int pi = 0; pi < 3; pi++) {
+            if constexpr (STAGE) {
+                if (pi == 1) { cp_async_wait<1>(); __syncthreads(); }
+                if (pi == 2) { cp_async_wait<0>(); __syncthreads(); }
+            }
+            k3_load_pair<T, L, E>(A, sbase + pi * sstride, false, sbase + (pi + 3) * sstride, false, g.Kz, sz, q, ok);
+            fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(A, sm, q, tw);
+            if (pi == 0) {
+#pragma unroll
+                for (int e = 0; e < E; e++) { rs[0][e] = A[e].x; rs[1][e] = A[e].y; }
+            } else if (pi == 1) {
+#pragma unroll
+                for (int e = 0; e < E; e++) { rs[2][e] = A[e].x; rs[3][e] = A[e].y; rs[4][e] = rs[1][e] * A[e].x - A[e].y * rs[0][e]; }
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+            const T uu = rs[0][e], ox = rs[1][e], vv = rs[2][e], oy = rs[3][e], ww = A[e].x, oz = A[e].y;
+            cfl_update<T>(mx, uu, vv, ww, c);
+            A[e] = mk<T>(oy * ww - oz * vv, oz * uu - ox * ww);
+        }
+        if (!ok) { mx[0] = mx[1] = mx[2] = mx[3] = 0.0; }
+        block_max4<T>(mx, ds);
+#pragma unroll 1
+        for (int j = 0; j < 2; j++) {
+            if (j == 1) {
+#pragma unroll
+                for (int e = 0; e < E; e++) A[e] = mk<T>(rs[4][e], T(0));
+            }
+            k3_store_job<T, L, E>(A, sm, q, g.Kz, j == 0 ? F(0) : F(2), j == 0 ? F(1) : nullptr, false, j == 1, sz, ok, tw);
+        }
+        } else {
         k3_load_pair<T, L, E>(A, src[0], false, src[3], false, g.Kz, sz, q, ok);
         fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(A, sm, q, tw);
         if constexpr (STAGE) { cp_async_wait<1>(); __syncthreads(); }
@@ -455,6 +509,7 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
         block_max4<T>(mx, ds);
         k3_store_pair<T, L, E>(A, sm, q, g.Kz, F(0), F(1), false, sz, ok, tw);
         k3_store_single<T, L, E>(B, sm, q, g.Kz, F(2), ok, tw);
+        }
     } else {
         // Advective form of the reference (src/HIT_LES.cpp:74-125): conv_i = u_j d_j u_i.
         // S2 inputs: 0 u, 1 v, 2 w, 3 du/dx, 4 dv/dx, 5 dw/dx, 6 du/dy, 7 dv/dy, 8 dw/dy;
@@ -467,6 +522,12 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
         // LES transforms overflow the instruction cache.
         cx<T> A[E];
         T rg[NREG > 0 ? NREG : 1][E];
+        // slots are written in one iteration of the pair loop and read in later ones:
+        // define them on entry (a rolled loop over partly defined registers miscompiled)
+#pragma unroll
+        for (int i = 0; i < (NREG > 0 ? NREG : 1); i++)
+#pragma unroll
+            for (int e = 0; e < E; e++) rg[i][e] = T(0);
 #define PH(slot, row) k3_slot<(slot), NREG, L, T, E>(rg, ph, e, row)
         // inverse pairs: (u, v), (w, du/dz), (du/dx, du/dy), (dv/dx, dv/dy), (dw/dx, dw/dy), (dv/dz, dw/dz)
 #pragma unroll 1

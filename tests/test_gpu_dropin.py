@@ -69,7 +69,7 @@ def test_reference_driver_qa(name, tmp_path):
         pytest.fail("drop-in driver not built (make -C spns_b200/dropin)")
     _stage(name, str(tmp_path))
     env = dict(os.environ, SPNS_K41_RANKS="4")
-    r = subprocess.run([EXE, "params"], cwd=str(tmp_path), env=env, capture_output=True, timeout=600)
+    r = subprocess.run([EXE, "params"], cwd=str(tmp_path), env=env, capture_output=True, timeout=120)
     out = r.stdout.decode(errors="replace") + r.stderr.decode(errors="replace")
     assert r.returncode == 0, out[-3000:]
     with open(os.path.join(str(tmp_path), "stdout.0"), errors="replace") as fh:
