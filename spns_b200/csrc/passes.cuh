@@ -37,7 +37,7 @@ template <typename T> struct Passes {
         using S3 = Shape3<T, L, MODE>;
         constexpr bool STAGE = MODE == spns::MODE_ROT && ShapeSel<T>::Z_STAGE;
         auto kern = spns::k3_z<T, L, S3::E, S3::P, MODE, STAGE>;
-        const size_t smem = S3::SMEM + (STAGE ? (size_t)S3::P * 6 * h->g.Kz * sizeof(C) : 0);
+        const size_t smem = S3::SMEM + (STAGE ? (size_t)S3::P * 2 * spns::K3StagePairs<T>::N * h->g.Kz * sizeof(C) : 0);
         cudaError_t e = spns_set_smem(kern, smem);
         if (e != cudaSuccess) return e;
         const long long npen = (long long)h->g.Mx * h->g.My;

@@ -354,12 +354,13 @@ template <int MODE> struct K3Phys { static constexpr int N = MODE == MODE_ADV ? 
 #ifndef SPNS_F32_K3_REG_SLOTS
 #define SPNS_F32_K3_REG_SLOTS 9
 #endif
-#ifndef SPNS_K3_ROT_LOOP
-#define SPNS_K3_ROT_LOOP 1    // double rotational z pass: one copy of the forward transform code
+#ifndef SPNS_Z_STAGE_PAIRS
+#define SPNS_Z_STAGE_PAIRS 3      // double rotational z pass: input pairs staged in shared memory
 #endif
-#ifndef SPNS_F32_K3_ROT_LOOP
-#define SPNS_F32_K3_ROT_LOOP 1
+#ifndef SPNS_F32_Z_STAGE_PAIRS
+#define SPNS_F32_Z_STAGE_PAIRS 3
 #endif
+template <typename T> struct K3StagePairs { static constexpr int N = sizeof(T) == 8 ? SPNS_Z_STAGE_PAIRS : SPNS_F32_Z_STAGE_PAIRS; };
 template <typename T, int MODE> struct K3Reg {
     static constexpr int R = sizeof(T) == 8 ? SPNS_K3_REG_SLOTS : SPNS_F32_K3_REG_SLOTS;
     static constexpr int N = K3Phys<MODE>::N < R ? K3Phys<MODE>::N : R;   // slots in registers
@@ -423,47 +424,48 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
         block_sum(ss, &ds->sumsq_phys);
     } else if constexpr (MODE == MODE_ROT) {
         // pairs (u, w_x), (v, w_y), (w, w_z);  c = w x u  (= u.grad u + gradient)
-        cx<T> A[E], B[E], C[E];
+        // STAGE: the input fields of the last NSP pairs are copied into shared memory
+        // asynchronously at the start, in the order the pairs use them, so their loads
+        // overlap the transforms of the earlier pairs.
+        constexpr int NSP = STAGE ? K3StagePairs<T>::N : 0;
+        constexpr int FIRST = 3 - NSP;
+        cx<T> A[E];
         const cx<T> *src[6] = {F(0), F(1), F(2), F(3), F(4), F(5)};
         if constexpr (STAGE) {
-            cx<T> *st = smc + P * SmPencil<T, L>::PITCH + (long long)p * 6 * g.Kz;
+            cx<T> *st = smc + P * SmPencil<T, L>::PITCH + (long long)p * 2 * NSP * g.Kz;
 #pragma unroll
-            for (int gp = 0; gp < 3; gp++) {
+            for (int gp = FIRST; gp < 3; gp++) {
 #pragma unroll
                 for (int h = 0; h < 2; h++) {
-                    const int f = gp + 3 * h;        // (0,3), (1,4), (2,5)
+                    const int f = gp + 3 * h, slot = 2 * (gp - FIRST) + h;
                     if (ok)
-                        for (int k = q; k < g.Kz; k += Q) cp_async_elem<T>(st + f * g.Kz + k, src[f] + k);
+                        for (int k = q; k < g.Kz; k += Q) cp_async_elem<T>(st + slot * g.Kz + k, src[f] + k);
                 }
                 cp_async_commit();
             }
 #pragma unroll
-            for (int f = 0; f < 6; f++) src[f] = st + f * g.Kz;
-            cp_async_wait<2>();
-            __syncthreads();
+            for (int gp = FIRST; gp < 3; gp++) {
+                src[gp] = st + 2 * (gp - FIRST) * g.Kz;
+                src[gp + 3] = st + (2 * (gp - FIRST) + 1) * g.Kz;
+            }
         }
-        constexpr bool ROT_LOOP = sizeof(T) == 8 ? SPNS_K3_ROT_LOOP : SPNS_F32_K3_ROT_LOOP;
-        if constexpr (ROT_LOOP) {
-        // one copy of the transform code: the pairs in a loop, physical values in register slots
-        // 0 u, 1 w_x, 2 v, 3 w_y, 4 c_z
-        (void)B; (void)C;
-        // The pair loop is unrolled (three transform copies; the two forward jobs share
-        // one): rolled, with slots written in one iteration and read in a later
-        // one, it computed wrong products.  The slots are defined on entry all the same.
+        // Physical values in register slots 0 u, 1 w_x, 2 v, 3 w_y, 4 c_z.  The pair
+        // loop is unrolled (rolled, with slots written in one iteration and read in a
+        // later one, it computed wrong products); the two forward jobs share one
+        // transform body.  The slots are defined on entry all the same.
         T rs[5][E];
 #pragma unroll
         for (int i = 0; i < 5; i++)
 #pragma unroll
             for (int e = 0; e < E; e++) rs[i][e] = T(0);
-        const cx<T> *sbase = src[0];
-        const long long sstride = src[1] - src[0];
 #pragma unroll
         for (int pi = 0; pi < 3; pi++) {
             if constexpr (STAGE) {
-                if (pi == 1) { cp_async_wait<1>(); __syncthreads(); }
-                if (pi == 2) { cp_async_wait<0>(); __syncthreads(); }
+                if (pi == FIRST) { cp_async_wait<NSP - 1>(); __syncthreads(); }
+                else if (pi == FIRST + 1) { cp_async_wait<(NSP >= 2 ? NSP - 2 : 0)>(); __syncthreads(); }
+                else if (pi == FIRST + 2) { cp_async_wait<0>(); __syncthreads(); }
             }
-            k3_load_pair<T, L, E>(A, sbase + pi * sstride, false, sbase + (pi + 3) * sstride, false, g.Kz, sz, q, ok);
+            k3_load_pair<T, L, E>(A, src[pi], false, src[pi + 3], false, g.Kz, sz, q, ok);
             fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(A, sm, q, tw);
             if (pi == 0) {
 #pragma unroll
@@ -488,27 +490,6 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
                 for (int e = 0; e < E; e++) A[e] = mk<T>(rs[4][e], T(0));
             }
             k3_store_job<T, L, E>(A, sm, q, g.Kz, j == 0 ? F(0) : F(2), j == 0 ? F(1) : nullptr, false, j == 1, sz, ok, tw);
-        }
-        } else {
-        k3_load_pair<T, L, E>(A, src[0], false, src[3], false, g.Kz, sz, q, ok);
-        fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(A, sm, q, tw);
-        if constexpr (STAGE) { cp_async_wait<1>(); __syncthreads(); }
-        k3_load_pair<T, L, E>(B, src[1], false, src[4], false, g.Kz, sz, q, ok);
-        fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(B, sm, q, tw);
-        if constexpr (STAGE) { cp_async_wait<0>(); __syncthreads(); }
-        k3_load_pair<T, L, E>(C, src[2], false, src[5], false, g.Kz, sz, q, ok);
-        fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(C, sm, q, tw);
-#pragma unroll
-        for (int e = 0; e < E; e++) {
-            const T uu = A[e].x, ox = A[e].y, vv = B[e].x, oy = B[e].y, ww = C[e].x, oz = C[e].y;
-            cfl_update<T>(mx, uu, vv, ww, c);
-            A[e] = mk<T>(oy * ww - oz * vv, oz * uu - ox * ww);
-            B[e] = mk<T>(ox * vv - oy * uu, T(0));
-        }
-        if (!ok) { mx[0] = mx[1] = mx[2] = mx[3] = 0.0; }
-        block_max4<T>(mx, ds);
-        k3_store_pair<T, L, E>(A, sm, q, g.Kz, F(0), F(1), false, sz, ok, tw);
-        k3_store_single<T, L, E>(B, sm, q, g.Kz, F(2), ok, tw);
         }
     } else {
         // Advective form of the reference (src/HIT_LES.cpp:74-125): conv_i = u_j d_j u_i.
