@@ -65,6 +65,21 @@ struct StepConsts {
 
 __device__ __forceinline__ int ffreq(int a, int M) { return a <= M / 2 ? a : a - M; }
 
+// Blocks per SM the x/y passes are compiled for (their register budget), per
+// pass (1 inverse x, 2 inverse y, 4 forward y, 5 forward x).
+#ifndef SPNS_AX_MINB
+#define SPNS_AX_MINB 2
+#endif
+#ifndef SPNS_K2_MINB
+#define SPNS_K2_MINB SPNS_AX_MINB
+#endif
+#ifndef SPNS_F32_AX_MINB
+#define SPNS_F32_AX_MINB 2
+#endif
+template <typename T, int PASS> struct AxisMinBlocks {
+    static constexpr int N = sizeof(T) == 8 ? ((PASS == 2 || PASS == 4) ? SPNS_K2_MINB : SPNS_AX_MINB) : SPNS_F32_AX_MINB;
+};
+
 // Field counts of the work buffers per mode.
 template <int MODE> struct Fields {
     static constexpr int K1 = MODE == MODE_VEL ? 3 : MODE == MODE_ROT ? 5 : 6;  // S1 after the inverse x pass
@@ -77,7 +92,7 @@ template <int MODE> struct Fields {
 //   VEL: u,v,w   ROT: u,v,w, w_y=i(kz u-kx w), i kx v   ADV/LES: u,v,w, du/dx, dv/dx, dw/dx
 // ===========================================================================
 template <typename T, int L, int E, int P, int MODE>
-__global__ void __launch_bounds__(P *(L / E), 2) k1_inv_x(Geo g, const cx<T> *__restrict__ u, const cx<T> *__restrict__ v,
+__global__ void __launch_bounds__(P *(L / E), AxisMinBlocks<T, 1>::N) k1_inv_x(Geo g, const cx<T> *__restrict__ u, const cx<T> *__restrict__ v,
                                                        const cx<T> *__restrict__ w, cx<T> *__restrict__ out,
                                                        const cx<T> *__restrict__ tw) {
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -126,7 +141,7 @@ __global__ void __launch_bounds__(P *(L / E), 2) k1_inv_x(Geo g, const cx<T> *__
 //   ADV/LES: u,v,w, du/dx,dv/dx,dw/dx, du/dy,dv/dy,dw/dy
 // ===========================================================================
 template <typename T, int L, int E, int P, int MODE>
-__global__ void __launch_bounds__(P *(L / E), 2) k2_inv_y(Geo g, const cx<T> *__restrict__ in, cx<T> *__restrict__ out,
+__global__ void __launch_bounds__(P *(L / E), AxisMinBlocks<T, 2>::N) k2_inv_y(Geo g, const cx<T> *__restrict__ in, cx<T> *__restrict__ out,
                                                        const cx<T> *__restrict__ tw) {
     extern __shared__ __align__(16) unsigned char smraw[];
     const int tid = threadIdx.x, p = tid % P, q = tid / P;
@@ -652,7 +667,7 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
 // LES: G_i += i ky t_i2 (SGS divergence, y part).
 // ===========================================================================
 template <typename T, int L, int E, int P, int MODE>
-__global__ void __launch_bounds__(P *(L / E), 2) k4_fwd_y(Geo g, const cx<T> *__restrict__ in, cx<T> *__restrict__ out,
+__global__ void __launch_bounds__(P *(L / E), AxisMinBlocks<T, 4>::N) k4_fwd_y(Geo g, const cx<T> *__restrict__ in, cx<T> *__restrict__ out,
                                                        const cx<T> *__restrict__ tw) {
     extern __shared__ __align__(16) unsigned char smraw[];
     const int tid = threadIdx.x, p = tid % P, q = tid / P;
@@ -712,7 +727,7 @@ __global__ void __launch_bounds__(P *(L / E), 2) k4_fwd_y(Geo g, const cx<T> *__
 // (S0).  Block = (kz chunk, iy).  LES: G_i += i kx t_i1 (SGS divergence, x part).
 // ===========================================================================
 template <typename T, int L, int E, int P, int MODE>
-__global__ void __launch_bounds__(P *(L / E), 2) k5_fwd_x(Geo g, const cx<T> *__restrict__ in, cx<T> *__restrict__ G,
+__global__ void __launch_bounds__(P *(L / E), AxisMinBlocks<T, 5>::N) k5_fwd_x(Geo g, const cx<T> *__restrict__ in, cx<T> *__restrict__ G,
                                                           const cx<T> *__restrict__ tw) {
     extern __shared__ __align__(16) unsigned char smraw[];
     const int tid = threadIdx.x, p = tid % P, q = tid / P;
