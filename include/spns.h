@@ -112,6 +112,15 @@ int spns_complex_conjugate_correction(spns_handle *h);
  * Fourier sum, the physical sum and the shell integral; *ok = all within atol. */
 int spns_check_physfour_energy(spns_handle *h, double atol, int *ok, double *diff1, double *diff2);
 
+/* HIT::Recalculate_Invariants_Distribution (src/HIT_LES.cpp:1297-1319, invariant
+ * definitions src/tensor_algebra.cpp:165-306, 356-358): spectra[c*(last_rad_max+1) + K]
+ * for c = Q_G, Q_S, R_G, R_S, V^2 of the velocity-gradient tensor G_ij = d_j u_i,
+ * each the shell integral of |F_c(k)|^2 (conjugate weight 2 for kz > 0) of the
+ * normalised transform.  Computed from the current spectral state (the reference
+ * uses the gradients of the last step's start).  The first call allocates work
+ * buffers of the advective step's size (6 S1 + 9 S2 fields), kept until destroy. */
+int spns_invariant_spectra(spns_handle *h, double *spectra);
+
 /* getters / HIT::setnu (src/HIT_LES.h:187-201) */
 int spns_get_scalars(spns_handle *h, spns_scalars *out);
 int spns_set_nu(spns_handle *h, double nu);

@@ -57,6 +57,7 @@ def lib():
             getattr(L, name).argtypes = [vp]
             getattr(L, name).restype = d
         L.orc_recalculate_energy_cascade.argtypes = [vp, dp]
+        L.orc_invariant_spectra.argtypes = [vp, dp]
         L.orc_recalculate_energy_cascade.restype = d
         L.orc_check_physfour_energy.argtypes = [vp, d, dp, dp]
         L.orc_check_physfour_energy.restype = i
@@ -136,6 +137,13 @@ class OracleHIT:
 
     def Recalculate_Enstrophy(self):
         return self._L.orc_recalculate_enstrophy(self._h)
+
+    def Recalculate_Invariants_Distribution(self):
+        """Spectra [5][last_rad_max+1] of Q_G, Q_S, R_G, R_S, V^2 (src/HIT_LES.cpp:1297-1319)."""
+        s = self._scalars()
+        out = np.zeros((5, int(s[12]) + 1))
+        self._L.orc_invariant_spectra(self._h, _dp(out))
+        return out
 
     def Recalculate_Energy_Cascade(self):
         s = self._scalars()

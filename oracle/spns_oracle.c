@@ -455,6 +455,83 @@ static void convective(orc *o) { /* :74-125 */
     }
 }
 
+/* Velocity-gradient invariants of G_ij = d_j u_i (src/HIT_LES.cpp:1297-1319 with
+ * the definitions of src/tensor_algebra.cpp:165-306, 356-358): Q_G, Q_S second
+ * invariants 1/2 (tr(T)^2 - tr(T T)) of G and of S = (G + G^T)/2; R_G, R_S their
+ * determinants; V^2 = 4 (tr(S^2 Omega^2) - 2 Q_S Q_Omega), Omega = G - S,
+ * Q_Omega = Q_G - Q_S. */
+static double second_invariant3(double T[3][3]) {
+    double tr = T[0][0] + T[1][1] + T[2][2], tr2 = 0.0;
+    for (int i = 0; i < 3; i++)
+        for (int k = 0; k < 3; k++) tr2 += T[i][k] * T[k][i];
+    return 0.5 * (tr * tr - tr2);
+}
+static double determinant3(double t[3][3]) {
+    double det = 0.0;
+    det += t[0][0] * t[1][1] * t[2][2];
+    det += t[0][1] * t[1][2] * t[2][0];
+    det += t[0][2] * t[1][0] * t[2][1];
+    det -= t[0][2] * t[1][1] * t[2][0];
+    det -= t[0][1] * t[1][0] * t[2][2];
+    det -= t[0][0] * t[1][2] * t[2][1];
+    return det;
+}
+static void grad_invariants(double G[3][3], double out[5]) {
+    double S[3][3], O[3][3], S2[3][3], O2[3][3];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) { S[i][j] = 0.5 * G[i][j] + 0.5 * G[j][i]; O[i][j] = G[i][j] - S[i][j]; }
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            S2[i][j] = 0.0; O2[i][j] = 0.0;
+            for (int k = 0; k < 3; k++) { S2[i][j] += S[i][k] * S[k][j]; O2[i][j] += O[i][k] * O[k][j]; }
+        }
+    double trS2O2 = 0.0;
+    for (int i = 0; i < 3; i++)
+        for (int k = 0; k < 3; k++) trS2O2 += S2[i][k] * O2[k][i];
+    const double QG = second_invariant3(G), QS = second_invariant3(S);
+    out[0] = QG;
+    out[1] = QS;
+    out[2] = determinant3(G);
+    out[3] = determinant3(S);
+    out[4] = 4.0 * (trS2O2 - 2.0 * QS * (QG - QS));
+}
+
+void orc_invariant_spectra(orc *o, double *out) {
+    velocity_gradients(o);
+    cplx **gks[3] = {o->gradu_k, o->gradv_k, o->gradw_k};
+    double **gs[3] = {o->gradu, o->gradv, o->gradw};
+    for (int c = 0; c < 3; c++)
+        for (int d = 0; d < 3; d++) fft_c2r(o, gks[c][d], gs[c][d]);
+    double *inv[5];
+    for (int c = 0; c < 5; c++) inv[c] = alloc_real(2 * o->alloc_local);
+    LOOP_REAL(o) {
+        long ind = IND_R(o);
+        double G[3][3], q[5];
+        for (int c = 0; c < 3; c++)
+            for (int d = 0; d < 3; d++) G[c][d] = gs[c][d][ind];
+        grad_invariants(G, q);
+        for (int c = 0; c < 5; c++) inv[c][ind] = q[c];
+    }
+    cplx *fk = alloc_complex(o->alloc_local);
+    const long nb = o->last_rad_max + 1;
+    for (int c = 0; c < 5; c++) {
+        fft_r2c(o, inv[c], fk);
+        fourier_normalization(o, fk);
+        double *acc = out + c * nb;
+        for (long K = 0; K < nb; K++) acc[K] = 0.0;
+        LOOP_FOURIER(o) {
+            long ind = IND_F(o);
+            if (!o->dealiased[ind]) continue;
+            int K = (int)round(sqrt(o->rad2[ind]));
+            if (K > o->last_rad_max) continue;
+            double aux = fk[ind][0] * fk[ind][0] + fk[ind][1] * fk[ind][1];
+            acc[K] += o->conjugate[ind] ? 2 * aux : aux;
+        }
+        free(inv[c]);
+    }
+    free(fk);
+}
+
 static void sgs_divergence(orc *o) { /* :130-192 */
     const double ct = o->C_Smag * o->C_Smag * o->delta * o->delta;
     double **gu = o->gradu, **gv = o->gradv, **gw = o->gradw;

@@ -137,6 +137,8 @@ struct spns_handle {
     int forced_cap = 0;
     double *phys = nullptr;
     void *edge = nullptr;                            // edge-correction planes (rotational form)
+    void *inv_B1 = nullptr, *inv_B2 = nullptr;       // invariant spectra: advective-size work buffers (on first use)
+    double *inv_bins = nullptr;
     bool edge_axis[3] = {false, false, false};       // axes whose +-N/2 planes alias (M = 3h)
     std::map<int, void *> tw;                        // twiddle tables per length (precision of the handle)
     std::string err;
@@ -226,6 +228,7 @@ struct PrecOps {
     int (*forcing_scale)(spns_handle *h, int last_eff, int nullify); // u *= FT[K]
     int (*conj_correction)(spns_handle *h);                   // kz=0 conjugate correction
     int (*seed_draw)(spns_handle *h, unsigned long long seed, int lim_x, int lim_y, int lim_z); // Philox field, unscaled
+    int (*invariant_spectra)(spns_handle *h, double *out);    // 5 spectra of the gradient invariants
 };
 extern const PrecOps spns_ops_f64;
 extern const PrecOps spns_ops_f32;

@@ -147,6 +147,46 @@ template <typename T> struct Passes {
         return SPNS_OK;
     }
 
+    // Spectra of the velocity-gradient invariants Q_G, Q_S, R_G, R_S, V^2 of the
+    // current state (Recalculate_Invariants_Distribution, src/HIT_LES.cpp:1297-1319):
+    // the five passes in MODE_INV on work buffers of the advective size (allocated
+    // on first use and kept; the step's own buffers and graphs are not touched),
+    // then shell sums of |F|^2 / (Mx My Mz)^2.  out[c*(last_rad_max+1) + K] on the host.
+    static int invariant_spectra(spns_handle *h, double *out) {
+        const spns::Geo &g = h->g;
+        const int nb = h->last_rad_max + 1;
+        if (!h->inv_B1) {
+            CK(cudaMallocAsync(&h->inv_B1, sizeof(C) * 6 * (size_t)g.S1, h->st));
+            CK(cudaMallocAsync(&h->inv_B2, sizeof(C) * 9 * (size_t)g.S2, h->st));
+            CK(cudaMallocAsync((void **)&h->inv_bins, sizeof(double) * 5 * nb, h->st));
+        }
+        std::swap(h->B1, h->inv_B1);
+        std::swap(h->B2, h->inv_B2);
+        auto passes = [&]() -> int {
+            DISPATCH(g.Mx, LAUNCH((launch_k1<LL, spns::MODE_INV>(h))));
+            DISPATCH(g.My, LAUNCH((launch_k2<LL, spns::MODE_INV>(h))));
+            DISPATCH(g.Mz, LAUNCH((launch_k3<LL, spns::MODE_INV>(h, nullptr))));
+            DISPATCH(g.My, LAUNCH((launch_k4<LL, spns::MODE_INV>(h))));
+            DISPATCH(g.Mx, LAUNCH((launch_k5<LL, spns::MODE_INV>(h))));
+            return SPNS_OK;
+        };
+        const int r = passes();
+        std::swap(h->B1, h->inv_B1);
+        std::swap(h->B2, h->inv_B2);
+        if (r) return r;
+        CK(cudaMemsetAsync(h->inv_bins, 0, sizeof(double) * 5 * nb, h->st));
+        const double scale = h->c.inv_norm * h->c.inv_norm;
+        const int blocks = (int)std::min<long long>((g.S0 + 255) / 256, 148 * 8);
+        for (int c = 0; c < 5; c++) {
+            spns::k_shell_sums_scalar<T><<<blocks, 256, sizeof(double) * nb, h->st>>>(
+                g, (const C *)h->inv_B2 + (long long)c * g.S0, scale, h->last_rad_max, h->inv_bins + (long long)c * nb);
+            CKL();
+        }
+        CK(cudaMemcpyAsync(out, h->inv_bins, sizeof(double) * 5 * nb, cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
+        return SPNS_OK;
+    }
+
     // Exact aliasing correction of the rotational form on the +-N/2 planes
     // (edge_kernels.cuh), added to the compact nonlinear term G held in B2.
     static int edge_correction(spns_handle *h) {
@@ -251,6 +291,6 @@ template <typename T> struct Passes {
     }
 
     static constexpr PrecOps ops() {
-        return PrecOps{&step_once, &run_velocity, &shell_sums, &forcing_scale, &conj_correction, &seed_draw};
+        return PrecOps{&step_once, &run_velocity, &shell_sums, &forcing_scale, &conj_correction, &seed_draw, &invariant_spectra};
     }
 };

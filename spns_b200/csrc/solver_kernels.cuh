@@ -29,7 +29,10 @@
 
 namespace spns {
 
-enum Mode { MODE_VEL = 0, MODE_ROT = 1, MODE_ADV = 2, MODE_LES = 3 };
+enum Mode { MODE_VEL = 0, MODE_ROT = 1, MODE_ADV = 2, MODE_LES = 3, MODE_INV = 4 };
+// MODE_INV: velocity-gradient invariants (post-processing, not a step): the x/y
+// passes form the gradients as in MODE_ADV, the z pass forms Q_G, Q_S, R_G, R_S, V^2
+// on the grid and transforms them forward, the forward y/x passes carry 5 fields.
 
 struct Geo {
     int Kx, Ky, Kz;   // retained mode counts
@@ -84,7 +87,8 @@ template <typename T, int PASS> struct AxisMinBlocks {
 template <int MODE> struct Fields {
     static constexpr int K1 = MODE == MODE_VEL ? 3 : MODE == MODE_ROT ? 5 : 6;  // S1 after the inverse x pass
     static constexpr int K2 = MODE == MODE_VEL ? 3 : MODE == MODE_ROT ? 6 : 9;  // S2 after the inverse y pass
-    static constexpr int K4 = MODE == MODE_LES ? 6 : 3;                         // S1 after the forward y pass
+    static constexpr int K4 = MODE == MODE_LES ? 6 : MODE == MODE_INV ? 5 : 3;  // S1 after the forward y pass
+    static constexpr int NOUT = MODE == MODE_INV ? 5 : 3;                       // compact outputs of the forward x pass
 };
 
 // ===========================================================================
@@ -359,7 +363,7 @@ template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile(
 
 // Shared-memory slots of physical fields kept per pencil (rows of this thread only).
 // slots: 0 u, 1 v, 2 w, 3..5 conv_x,y,z, LES 6..11 a11, a12, a22, a13, a23, a33 (then t_ij)
-template <int MODE> struct K3Phys { static constexpr int N = MODE == MODE_ADV ? 6 : MODE == MODE_LES ? 12 : 0; };
+template <int MODE> struct K3Phys { static constexpr int N = MODE == MODE_ADV ? 6 : MODE == MODE_LES ? 12 : MODE == MODE_INV ? 9 : 0; };
 // The first slots live in registers (indexed by the thread's register slot e, not
 // by row), the rest in shared memory: the twelve LES slots of a 384-pencil take
 // 37 KB of shared memory in FP64, which alone would allow 4 pencils per SM.
@@ -506,6 +510,110 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
             }
             k3_store_job<T, L, E>(A, sm, q, g.Kz, j == 0 ? F(0) : F(2), j == 0 ? F(1) : nullptr, false, j == 1, sz, ok, tw);
         }
+    } else if constexpr (MODE == MODE_INV) {
+        // Velocity-gradient invariants (src/HIT_LES.cpp:1297-1319, definitions
+        // src/tensor_algebra.cpp:165-306, 356-358) of G_ij = d_j u_i.
+        // S2 inputs as in the advective form: 0 u, 1 v, 2 w, 3 du/dx, 4 dv/dx, 5 dw/dx,
+        // 6 du/dy, 7 dv/dy, 8 dw/dy; z-derivatives formed here.  Slots s = 3 i + j hold G_ij.
+        // Outputs (S2 fields 0..4): Q_G, Q_S, R_G, R_S, V^2 forward-transformed, kz <= hz.
+        cx<T> A[E];
+        T rg[NREG > 0 ? NREG : 1][E];
+#pragma unroll
+        for (int i = 0; i < (NREG > 0 ? NREG : 1); i++)
+#pragma unroll
+            for (int e = 0; e < E; e++) rg[i][e] = T(0);
+#define PH(slot, row) k3_slot<(slot), NREG, L, T, E>(rg, ph, e, row)
+        // pairs: (du/dx, du/dy), (dv/dx, dv/dy), (dw/dx, dw/dy), (du/dz, dv/dz), (dw/dz, -)
+#pragma unroll 1
+        for (int pi = 0; pi < 5; pi++) {
+            const cx<T> *fa = pi < 3 ? F(3 + pi) : pi == 3 ? F(0) : F(2);
+            const cx<T> *fb = pi < 3 ? F(6 + pi) : pi == 3 ? F(1) : nullptr;
+            k3_load_pair<T, L, E>(A, fa, pi >= 3, fb, pi == 3, g.Kz, sz, q, ok);
+            fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(A, sm, q, tw);
+            switch (pi) {
+            case 0:
+#pragma unroll
+                for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); PH(0, row) = A[e].x; PH(1, row) = A[e].y; }
+                break;
+            case 1:
+#pragma unroll
+                for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); PH(3, row) = A[e].x; PH(4, row) = A[e].y; }
+                break;
+            case 2:
+#pragma unroll
+                for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); PH(6, row) = A[e].x; PH(7, row) = A[e].y; }
+                break;
+            case 3:
+#pragma unroll
+                for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); PH(2, row) = A[e].x; PH(5, row) = A[e].y; }
+                break;
+            default:
+#pragma unroll
+                for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); PH(8, row) = A[e].x; }
+                break;
+            }
+        }
+        // invariants per grid row, written over slots 0..4
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+            const int row = out_row<L, E, true>(q, e);
+            double G[3][3], S[3][3], O[3][3], S2[3][3], O2[3][3];
+            G[0][0] = PH(0, row); G[0][1] = PH(1, row); G[0][2] = PH(2, row);
+            G[1][0] = PH(3, row); G[1][1] = PH(4, row); G[1][2] = PH(5, row);
+            G[2][0] = PH(6, row); G[2][1] = PH(7, row); G[2][2] = PH(8, row);
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) { S[i][j] = 0.5 * G[i][j] + 0.5 * G[j][i]; O[i][j] = G[i][j] - S[i][j]; }
+            double trG = G[0][0] + G[1][1] + G[2][2], trS = S[0][0] + S[1][1] + S[2][2], trGG = 0.0, trSS = 0.0, trS2O2 = 0.0;
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    trGG += G[i][j] * G[j][i];
+                    trSS += S[i][j] * S[j][i];
+                    double s2 = 0.0, o2 = 0.0;
+#pragma unroll
+                    for (int k = 0; k < 3; k++) { s2 += S[i][k] * S[k][j]; o2 += O[i][k] * O[k][j]; }
+                    S2[i][j] = s2; O2[i][j] = o2;
+                }
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int k = 0; k < 3; k++) trS2O2 += S2[i][k] * O2[k][i];
+            auto det3 = [](const double (&t)[3][3]) {
+                double d = 0.0;
+                d += t[0][0] * t[1][1] * t[2][2];
+                d += t[0][1] * t[1][2] * t[2][0];
+                d += t[0][2] * t[1][0] * t[2][1];
+                d -= t[0][2] * t[1][1] * t[2][0];
+                d -= t[0][1] * t[1][0] * t[2][2];
+                d -= t[0][0] * t[1][2] * t[2][1];
+                return d;
+            };
+            const double QG = 0.5 * (trG * trG - trGG), QS = 0.5 * (trS * trS - trSS);
+            PH(0, row) = T(QG);
+            PH(1, row) = T(QS);
+            PH(2, row) = T(det3(G));
+            PH(3, row) = T(det3(S));
+            PH(4, row) = T(4.0 * (trS2O2 - 2.0 * QS * (QG - QS)));
+        }
+#pragma unroll 1
+        for (int j = 0; j < 3; j++) {
+            if (j == 0) {
+#pragma unroll
+                for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(PH(0, row), PH(1, row)); }
+            } else if (j == 1) {
+#pragma unroll
+                for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(PH(2, row), PH(3, row)); }
+            } else {
+#pragma unroll
+                for (int e = 0; e < E; e++) { const int row = out_row<L, E, true>(q, e); A[e] = mk<T>(PH(4, row), T(0)); }
+            }
+            k3_store_job<T, L, E>(A, sm, q, g.Kz, F(2 * j), j < 2 ? F(2 * j + 1) : nullptr, false, j == 2, sz, ok, tw);
+        }
+        (void)mx;
+#undef PH
     } else {
         // Advective form of the reference (src/HIT_LES.cpp:74-125): conv_i = u_j d_j u_i.
         // S2 inputs: 0 u, 1 v, 2 w, 3 du/dx, 4 dv/dx, 5 dw/dx, 6 du/dy, 7 dv/dy, 8 dw/dy;
@@ -696,7 +804,7 @@ __global__ void __launch_bounds__(P *(L / E), AxisMinBlocks<T, 4>::N) k4_fwd_y(G
     };
     if constexpr (MODE != MODE_LES) {
 #pragma unroll 1
-        for (int f = 0; f < 3; f++) {
+        for (int f = 0; f < Fields<MODE>::NOUT; f++) {
             cx<T> r[E];
             load_fft(r, f);
             store(r, f, r, false);
@@ -742,7 +850,7 @@ __global__ void __launch_bounds__(P *(L / E), AxisMinBlocks<T, 5>::N) k5_fwd_x(G
         fft<T, L, E, false>(r, sm, q, tw);
     };
 #pragma unroll 1
-    for (int f = 0; f < 3; f++) {
+    for (int f = 0; f < Fields<MODE>::NOUT; f++) {
         cx<T> r[E];
         load_fft(r, f);
         if constexpr (MODE == MODE_LES) {
@@ -981,6 +1089,34 @@ __global__ void k_shell_sums(Geo g, const cx<T> *__restrict__ u, const cx<T> *__
         if (hE[i] != 0.0) atomicAdd(&Ek[i], hE[i]);
         if (hO[i] != 0.0) atomicAdd(&Om[i], hO[i]);
     }
+}
+
+// Shell sums of |F|^2 (conjugate weight 2 for kz>0), scaled by `scale`: the
+// spectrum of one scalar field (src/HIT_LES.cpp:1137-1214 with the integrands of
+// the invariant spectra, :1006-1025).
+template <typename T>
+__global__ void k_shell_sums_scalar(Geo g, const cx<T> *__restrict__ F, double scale, int Kmax, double *__restrict__ out) {
+    extern __shared__ double hist[];
+    for (int i = threadIdx.x; i <= Kmax; i += blockDim.x) hist[i] = 0.0;
+    __syncthreads();
+    const long long n = g.S0;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long long)gridDim.x * blockDim.x) {
+        const int kz = (int)(idx % g.Kz);
+        const long long t = idx / g.Kz;
+        const int ix = (int)(t % g.Kx), iy = (int)(t / g.Kx);
+        const long long k1 = (long long)g.sx * (ix <= g.hx ? ix : ix - g.Kx);
+        const long long k2 = (long long)g.sy * (iy <= g.hy ? iy : iy - g.Ky);
+        const long long k3 = (long long)g.sz * kz;
+        const int K = (int)round(sqrt((double)(k1 * k1 + k2 * k2 + k3 * k3)));
+        if (K > Kmax) continue;
+        const cx<T> a = F[idx];
+        double e = scale * ((double)a.x * a.x + (double)a.y * a.y);
+        if (kz != 0) e *= 2.0;
+        atomicAdd(&hist[K], e);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i <= Kmax; i += blockDim.x)
+        if (hist[i] != 0.0) atomicAdd(&out[i], hist[i]);
 }
 
 // Totals of the shell sums: Ek_Tot over K=0..Kmax, Ok_Tot over K=1..Kmax.

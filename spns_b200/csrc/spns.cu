@@ -321,7 +321,8 @@ static void free_handle(spns_handle *h) {
     if (!h) return;
     // stream-ordered frees: no device-wide synchronisation, so other handles'
     // work in flight (a serving loop) keeps running while this one is released
-    void *bufs[] = {h->ds, h->U, h->Ulo, h->R, h->Up, h->Uplo, h->B1, h->B2, h->bins, h->FT, h->forced, h->phys, h->edge};
+    void *bufs[] = {h->ds, h->U, h->Ulo, h->R, h->Up, h->Uplo, h->B1, h->B2, h->bins, h->FT, h->forced, h->phys, h->edge,
+                    h->inv_B1, h->inv_B2, h->inv_bins};
     for (void *b : bufs)
         if (b) cudaFreeAsync(b, h->st);
     for (auto &kv : h->tw) cudaFreeAsync(kv.second, h->st);
@@ -714,6 +715,11 @@ int spns_profile_read(spns_handle *h, float *ms, int cap, int *nkernels, int *ns
 const char *spns_profile_kernel_name(spns_handle *h, int i) {
     if (!h || i < 0 || i >= (int)h->prof_names.size()) return "";
     return h->prof_names[i].c_str();
+}
+
+int spns_invariant_spectra(spns_handle *h, double *spectra) {
+    if (!h || !spectra) return SPNS_ERR_INVALID_ARGUMENT;
+    return spns_ops(h).invariant_spectra(h, spectra);
 }
 
 int spns_estimate_device_bytes(const spns_hit_args *args, size_t *bytes) {

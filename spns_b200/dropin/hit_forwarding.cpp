@@ -242,11 +242,20 @@ void HIT::Check_PhysFour_Energy(const REAL atol) {
     if (!ok) crash("Ek differences exceed tolerance [EkReal vs EkFour %e, EkSpNS vs EkFour: %e]\n", d1, d2);
 }
 
-// Velocity-gradient invariant spectra (src/HIT_LES.cpp:1297-1319) are not part
-// of the GPU time step; a driver that asks for them stops here.
+// src/HIT_LES.cpp:1297-1319: spectra of Q_G, Q_S, R_G, R_S and V^2 of the
+// velocity-gradient tensor, each written as "K<TAB>value" lines (the format of
+// src/HIT_LES.cpp:1180-1187) when its file name is given.  They are computed
+// from the current spectral state.
 void HIT::Recalculate_Invariants_Distribution(const char *filename[5]) {
-    (void)filename;
-    crash("libspns drop-in: VelGradInv_Spectra output is not available on the GPU path");
+    std::vector<double> sp(5 * (size_t)(last_rad_max + 1));
+    SPNS_FORWARD(spns_invariant_spectra(h, sp.data()), "Recalculate_Invariants_Distribution");
+    if (!filename) return;
+    for (int c = 0; c < 5; c++) {
+        if (!filename[c]) continue;
+        std::ofstream out(filename[c]);
+        if (!out.is_open()) printf("WARNING: HIT::Integrate_Field(): Error opening \"%s\".\n", filename[c]);
+        for (ptrdiff_t K = 0; K <= last_rad_max; K++) out << K << "\t" << sp[c * (size_t)(last_rad_max + 1) + K] << "\n";
+    }
 }
 
 // src/HIT_LES_output.cpp:8-10, 20-64: the retained Fourier coefficients of

@@ -33,6 +33,7 @@ EXPORTED_SYMBOLS = (
     "spns_energy_cascade_noalloc_f64", "spns_estimate_device_bytes", "spns_seed_field", "spns_step_async",
     "spns_query", "spns_synchronize", "spns_checkpoint_bytes", "spns_checkpoint_save", "spns_checkpoint_load",
     "spns_ensemble_create", "spns_ensemble_step", "spns_ensemble_destroy", "spns_ensemble_last_error",
+    "spns_invariant_spectra",
 )
 
 
@@ -130,6 +131,7 @@ def lib():
         L.spns_ensemble_destroy.argtypes = [vp]
         L.spns_ensemble_last_error.argtypes = [vp]
         L.spns_ensemble_last_error.restype = C.c_char_p
+        L.spns_invariant_spectra.argtypes = [vp, dp]
         _lib = L
     return _lib
 
@@ -277,6 +279,18 @@ class HIT:
         tot = C.c_double()
         self._ck(self._L.spns_recalculate_energy_cascade(self._h, _dp(ek), C.byref(tot)))
         return ek
+
+    def Recalculate_Invariants_Distribution(self, filenames=None) -> np.ndarray:
+        """Spectra [5][last_rad_max+1] of Q_G, Q_S, R_G, R_S, V^2 (src/HIT_LES.cpp:1297-1319);
+        with five file names, each is written as ``K<TAB>value`` lines (src/HIT_LES.cpp:1180-1187)."""
+        out = np.zeros((5, self.getlast_rad_max() + 1))
+        self._ck(self._L.spns_invariant_spectra(self._h, _dp(out)))
+        if filenames is not None:
+            for name, sp in zip(filenames, out):
+                with open(name, "w") as fh:
+                    for K, v in enumerate(sp):
+                        fh.write(f"{K}\t{v:g}\n")
+        return out
 
     def Check_PhysFour_Energy(self, atol: float = 1e-13):
         ok, d1, d2 = C.c_int(), C.c_double(), C.c_double()
