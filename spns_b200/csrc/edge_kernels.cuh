@@ -132,11 +132,11 @@ __global__ void __launch_bounds__(P *(L / E)) k_lines(cx<T> *__restrict__ data, 
     const long long line = (long long)blockIdx.x * P + p;
     const bool ok = line < batch;
     cx<T> *d = data + (ok ? line : 0) * L;
-    SmPencil<T, L> sm{reinterpret_cast<cx<T> *>(smraw) + p * SmPencil<T, L>::PITCH};
+    SmPencil<T, L, E> sm{reinterpret_cast<cx<T> *>(smraw) + p * SmPencil<T, L, E>::PITCH};
     cx<T> r[E];
 #pragma unroll
     for (int e = 0; e < E; e++) r[e] = ok ? d[in_row<L, E, INV>(q, e)] : zero<T>();
-    fft<T, L, E, INV, SmPencil<T, L>, (32 % (L / E) == 0)>(r, sm, q, tw);
+    fft<T, L, E, INV, SmPencil<T, L, E>, (32 % (L / E) == 0)>(r, sm, q, tw);
     if (ok)
 #pragma unroll
         for (int e = 0; e < E; e++) d[out_row<L, E, INV>(q, e)] = r[e];

@@ -26,6 +26,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "fft_layouts.h"
+
 namespace spns {
 
 template <typename T> struct alignas(2 * sizeof(T)) cx { T x, y; };
@@ -161,6 +163,14 @@ template <typename T, int R, bool INV> __device__ __forceinline__ void dft(cx<T>
 // v[m*R + r] holds the input (before the stage) / output (after) of butterfly
 // j = q + Q*m, leg r.  WARP: the threads of a pencil exchange within one warp.
 // ---------------------------------------------------------------------------
+template <class SM, class = void> struct SmPadded { static constexpr bool value = false; };
+template <class SM> struct SmPadded<SM, decltype((void)SM::PADDED)> { static constexpr bool value = SM::PADDED; };
+// layout of exchange S of a padded accessor (pad >= 0, or -1 for the XOR swizzle); 0 for the others
+template <class SM, bool INV, int S> __host__ __device__ constexpr int ex_pad() {
+    if constexpr (SmPadded<SM>::value) return SM::template Ex<INV, S>::PAD;
+    else return 0;
+}
+
 template <bool WARP> __device__ __forceinline__ void stage_barrier() {
     if constexpr (WARP) __syncwarp(); else __syncthreads();
 }
@@ -192,23 +202,74 @@ __device__ __forceinline__ void fft_run(cx<T> (&v)[E], SM sm, int q, const cx<T>
         dft<T, R, INV>(&v[m * R]);
     }
     if constexpr (S + 1 < PL::NST) {
-#pragma unroll
-        for (int m = 0; m < MB; m++) {
-            const int j = q + Q * m;
-            const int base = (j / Ns) * Ns * R + (j % Ns);
-#pragma unroll
-            for (int r = 0; r < R; r++) sm.at(base + r * Ns) = v[m * R + r];
-        }
-        stage_barrier<WARP>();
         constexpr int R2 = PL::radix(S + 1);
         constexpr int MB2 = E / R2;
+        if constexpr (ex_pad<SM, INV, S>() < 0) {
+            // XOR-swizzled layout (fewer bank conflicts for this exchange)
 #pragma unroll
-        for (int m = 0; m < MB2; m++) {
-            const int j = q + Q * m;
+            for (int m = 0; m < MB; m++) {
+                const int j = q + Q * m;
+                const int base = (j / Ns) * Ns * R + (j % Ns);
 #pragma unroll
-            for (int r = 0; r < R2; r++) v[m * R2 + r] = sm.at(j + r * (L / R2));
+                for (int r = 0; r < R; r++) sm.xr(base + r * Ns) = v[m * R + r];
+            }
+            stage_barrier<WARP>();
+#pragma unroll
+            for (int m = 0; m < MB2; m++) {
+                const int j = q + Q * m;
+#pragma unroll
+                for (int r = 0; r < R2; r++) v[m * R2 + r] = sm.xr(j + r * (L / R2));
+            }
+            stage_barrier<WARP>();
+        } else if constexpr (SmPadded<SM>::value) {
+            // padded layout: one base address per butterfly group, offsets in the instructions
+            constexpr int X = Ns * R, PAD = SM::template Ex<INV, S>::PAD, XP = X + PAD;
+            cx<T> *const b = sm.base;
+#pragma unroll
+            for (int m = 0; m < MB; m++) {
+                cx<T> *w;
+                if constexpr (Q % Ns == 0) {
+                    w = b + (q / Ns) * XP + (q % Ns) + m * (Q / Ns) * XP;
+                } else {
+                    const int j = q + Q * m, hi = j / Ns;
+                    w = b + hi * XP + (j - hi * Ns);
+                }
+#pragma unroll
+                for (int r = 0; r < R; r++) w[r * Ns] = v[m * R + r];
+            }
+            stage_barrier<WARP>();
+            constexpr int STEP = L / R2, PSTEP = STEP + (STEP / X) * PAD;
+            static_assert(STEP % X == 0, "exchange read stride must be a multiple of the pad block");
+#pragma unroll
+            for (int m = 0; m < MB2; m++) {
+                const cx<T> *rd;
+                if constexpr (Q % X == 0) {
+                    rd = b + q + (q / X) * PAD + m * (Q + (Q / X) * PAD);
+                } else {
+                    const int row = q + Q * m;
+                    rd = b + row + (row / X) * PAD;
+                }
+#pragma unroll
+                for (int r = 0; r < R2; r++) v[m * R2 + r] = rd[r * PSTEP];
+            }
+            stage_barrier<WARP>();
+        } else {
+#pragma unroll
+            for (int m = 0; m < MB; m++) {
+                const int j = q + Q * m;
+                const int base = (j / Ns) * Ns * R + (j % Ns);
+#pragma unroll
+                for (int r = 0; r < R; r++) sm.at(base + r * Ns) = v[m * R + r];
+            }
+            stage_barrier<WARP>();
+#pragma unroll
+            for (int m = 0; m < MB2; m++) {
+                const int j = q + Q * m;
+#pragma unroll
+                for (int r = 0; r < R2; r++) v[m * R2 + r] = sm.at(j + r * (L / R2));
+            }
+            stage_barrier<WARP>();
         }
-        stage_barrier<WARP>();
         fft_run<T, L, E, INV, WARP, S + 1, SM>(v, sm, q, tw);
     }
 }
@@ -242,19 +303,47 @@ template <typename T, int P> struct SmRowMajor {
     cx<T> *base; int p;
     __device__ __forceinline__ cx<T> &at(int row) const { return base[row * P + p]; }
 };
-// Accessor: pencil-major [p][PITCH] with an XOR swizzle of the low row bits
-// by the bits two places up (G = 8 rows of 16 bytes, or 16 rows of 8 bytes =
-// one 128-byte bank line).  It maps each aligned block of G rows onto itself,
-// so PITCH is L rounded up to a multiple of G.  For the strides of the
-// Stockham exchanges (R*Ns apart on write, L/R apart on read) it spreads a
-// quarter-warp (double) or half-warp (float) over distinct banks in nearly
-// every stage; a padding of one slot per 8 rows left some stages 2-way
-// conflicted (double) or all of them (float).
-template <typename T, int L> struct SmPencil {
+// Accessor: pencil-major [p][PITCH], rows stored in order (post-processing
+// reads rows k and L-k of consecutive k: conflict-free as is).  The Stockham
+// exchanges of fft_run use their own padded layouts inside the same buffer
+// (PencilLayout below), so `at` is only for accesses outside the transform.
+template <typename T, int L, int E> struct SmPencil;
+
+// ---------------------------------------------------------------------------
+// Padded exchange layouts of the pencil-major buffer.
+//
+// Exchange S (written by stage S: radix R, span Ns; read by stage S+1: radix
+// R2) stores row r at  r + (r / X) * PAD  with X = Ns*R.  A butterfly's R
+// writes  (j/Ns)*X + j%Ns + r*Ns  all lie in one block of X rows, and the
+// reads  q + Q*m + r2*(L/R2)  step by multiples of X (L/R2 = X * the radices
+// after S+1), so every access of a thread is one base address plus
+// compile-time offsets: no per-access index arithmetic.  PAD per exchange and
+// the pencil pitch come from fft_layouts.h, generated by gen_layouts.py, which
+// counts the shared-memory wavefronts of each exchange's writes and reads; where
+// the XOR swizzle below has fewer, the table selects it (PAD = -1) and that
+// exchange pays per-access index arithmetic instead.
+// ---------------------------------------------------------------------------
+template <typename T, int L, int E> struct SmPencil {
     cx<T> *base;
-    static constexpr int G = sizeof(cx<T>) == 16 ? 8 : 16;
-    static constexpr int PITCH = (L + G - 1) / G * G;
-    __device__ __forceinline__ cx<T> &at(int row) const { return base[row ^ ((row >> 2) & (G - 1))]; }
+    static constexpr bool PADDED = true;
+    static constexpr int WPL = (int)(sizeof(cx<T>) / 4);
+    static constexpr int PITCH = exch::table_pitch(WPL, L, E);
+    static_assert(PITCH >= L, "no exchange layout generated for this length and E (gen_layouts.py)");
+    static constexpr int G = WPL == 4 ? 8 : 16;   // rows of one 128-byte bank line
+    // layout of exchange S of the inverse (INV) or forward plan: pad >= 0, or -1 for the XOR swizzle
+    template <bool INV, int S> struct Ex {
+#ifdef SPNS_EXCH_XOR_ONLY
+        static constexpr int PAD = -1;
+#else
+        static constexpr int PAD = exch::table_pad(WPL, L, E, INV, S);
+#endif
+        static_assert(PAD >= -1, "no exchange layout generated for this stage (gen_layouts.py)");
+        static_assert((PAD < 0 ? (L + G - 1) / G * G : L + (L / (Plan<L, E, INV>::ns(S) * Plan<L, E, INV>::radix(S))) * PAD) <= PITCH,
+                      "exchange layout exceeds the pencil pitch");
+    };
+    __device__ __forceinline__ cx<T> &at(int row) const { return base[row]; }
+    // XOR swizzle of the low row bits by the bits two places up; maps each aligned block of G rows onto itself
+    __device__ __forceinline__ cx<T> &xr(int row) const { return base[row ^ ((row >> 2) & (G - 1))]; }
 };
 
 } // namespace spns

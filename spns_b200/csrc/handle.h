@@ -34,7 +34,7 @@ template <typename T, int L, int E_, int THR> struct ShapeT {
     static constexpr int P = P0 >= 32 ? 32 : P0 >= 16 ? 16 : P0 >= 8 ? 8 : 4; // pencils per block
     static constexpr int THREADS = P * Q;
     static constexpr size_t SMEM_ROW = (size_t)L * P * sizeof(spns::cx<T>);
-    static constexpr size_t SMEM_PEN = (size_t)spns::SmPencil<T, L>::PITCH * P * sizeof(spns::cx<T>);
+    static constexpr size_t SMEM_PEN = (size_t)spns::SmPencil<T, L, E_>::PITCH * P * sizeof(spns::cx<T>);
 };
 // Double precision shapes (E, threads per block); single precision has its own
 // (half the register and shared-memory footprint per value).
@@ -104,7 +104,7 @@ template <typename T, int L, int MODE> struct Shape3 {
     static constexpr int Q = L / E;
     static constexpr int ZT = ShapeSel<T>::Z_T / Q;
     static constexpr int P0 = ZT >= 32 ? 32 : ZT >= 16 ? 16 : ZT >= 8 ? 8 : ZT >= 4 ? 4 : ZT >= 2 ? 2 : 1;
-    static constexpr size_t PER_PEN = (size_t)spns::SmPencil<T, L>::PITCH * sizeof(spns::cx<T>) + (size_t)spns::K3Reg<T, MODE>::NSM * L * sizeof(T);
+    static constexpr size_t PER_PEN = (size_t)spns::SmPencil<T, L, E>::PITCH * sizeof(spns::cx<T>) + (size_t)spns::K3Reg<T, MODE>::NSM * L * sizeof(T);
     static constexpr int PMAX = (int)((200 * 1024) / PER_PEN);
     static constexpr int P = P0 <= PMAX ? P0 : PMAX >= 16 ? 16 : PMAX >= 8 ? 8 : PMAX >= 4 ? 4 : PMAX >= 2 ? 2 : 1;
     static constexpr int THREADS = P * Q;

@@ -271,10 +271,10 @@ __device__ __forceinline__ void block_sum(double v, double *dst) {
 // half spectra for kz < Kz:  Xa = (Z_k + conj Z_{L-k})/2, Xb = (Z_k - conj Z_{L-k})/(2i).
 // With jz: Xa += i kz Xb (the z-derivative of b folded into a; SGS divergence).
 template <typename T, int L, int E>
-__device__ __forceinline__ void k3_store_pair(cx<T> (&r)[E], SmPencil<T, L> sm, int q, int Kz, cx<T> *A, cx<T> *B,
+__device__ __forceinline__ void k3_store_pair(cx<T> (&r)[E], SmPencil<T, L, E> sm, int q, int Kz, cx<T> *A, cx<T> *B,
                                               bool fold_dz_b_into_a, T sz, bool ok, const cx<T> *__restrict__ tw) {
     constexpr int Q = L / E;
-    fft<T, L, E, false, SmPencil<T, L>, (32 % (L / E) == 0)>(r, sm, q, tw);
+    fft<T, L, E, false, SmPencil<T, L, E>, (32 % (L / E) == 0)>(r, sm, q, tw);
 #pragma unroll
     for (int e = 0; e < E; e++) sm.at(out_row<L, E, false>(q, e)) = r[e];
     __syncthreads();
@@ -294,9 +294,9 @@ __device__ __forceinline__ void k3_store_pair(cx<T> (&r)[E], SmPencil<T, L> sm, 
 
 // Single real field: forward transform of (a + 0i), kz < Kz written directly.
 template <typename T, int L, int E>
-__device__ __forceinline__ void k3_store_single(cx<T> (&r)[E], SmPencil<T, L> sm, int q, int Kz, cx<T> *A, bool ok,
+__device__ __forceinline__ void k3_store_single(cx<T> (&r)[E], SmPencil<T, L, E> sm, int q, int Kz, cx<T> *A, bool ok,
                                                 const cx<T> *__restrict__ tw) {
-    fft<T, L, E, false, SmPencil<T, L>, (32 % (L / E) == 0)>(r, sm, q, tw);
+    fft<T, L, E, false, SmPencil<T, L, E>, (32 % (L / E) == 0)>(r, sm, q, tw);
     if (ok) {
 #pragma unroll
         for (int e = 0; e < E; e++) {
@@ -309,10 +309,10 @@ __device__ __forceinline__ void k3_store_single(cx<T> (&r)[E], SmPencil<T, L> sm
 // One forward job of the z pass: a pair (k3_store_pair) or, with `single`, a
 // single real field (k3_store_single), behind one copy of the transform code.
 template <typename T, int L, int E>
-__device__ __forceinline__ void k3_store_job(cx<T> (&r)[E], SmPencil<T, L> sm, int q, int Kz, cx<T> *A, cx<T> *B, bool fold,
+__device__ __forceinline__ void k3_store_job(cx<T> (&r)[E], SmPencil<T, L, E> sm, int q, int Kz, cx<T> *A, cx<T> *B, bool fold,
                                              bool single, T sz, bool ok, const cx<T> *__restrict__ tw) {
     constexpr int Q = L / E;
-    fft<T, L, E, false, SmPencil<T, L>, (32 % (L / E) == 0)>(r, sm, q, tw);
+    fft<T, L, E, false, SmPencil<T, L, E>, (32 % (L / E) == 0)>(r, sm, q, tw);
     if (single) {
         if (ok) {
 #pragma unroll
@@ -396,8 +396,28 @@ __device__ __forceinline__ T &k3_slot(T (&rg)[NREG > 0 ? NREG : 1][E], T *ph, in
 // three pairs use them, so the loads of the second and third pairs overlap the
 // transforms of the first.  Dynamic shared memory then holds P*6*Kz extra
 // complex values after the exchange buffers.
+// Minimum resident blocks per SM of the z pass (the register budget ptxas
+// allocates to): single precision 4 blocks (128 registers) for the velocity and
+// rotational forms, 3 for the advective and LES forms; double precision 1.
+#ifndef SPNS_K3_MINB_ROT
+#define SPNS_K3_MINB_ROT 1
+#endif
+#ifndef SPNS_K3_MINB_ADV
+#define SPNS_K3_MINB_ADV 1
+#endif
+#ifndef SPNS_F32_K3_MINB_ROT
+#define SPNS_F32_K3_MINB_ROT 4
+#endif
+#ifndef SPNS_F32_K3_MINB_ADV
+#define SPNS_F32_K3_MINB_ADV 3
+#endif
+template <typename T, int MODE> struct K3MinBlocks {
+    static constexpr bool D = sizeof(T) == 8;
+    static constexpr int N = (MODE == MODE_LES || MODE == MODE_ADV) ? (D ? SPNS_K3_MINB_ADV : SPNS_F32_K3_MINB_ADV)
+                           : (MODE == MODE_ROT || MODE == MODE_VEL) ? (D ? SPNS_K3_MINB_ROT : SPNS_F32_K3_MINB_ROT) : 1;
+};
 template <typename T, int L, int E, int P, int MODE, bool STAGE = false>
-__global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ buf, StepConsts c, DevScalars *ds,
+__global__ void __launch_bounds__(P *(L / E), K3MinBlocks<T, MODE>::N) k3_z(Geo g, cx<T> *__restrict__ buf, StepConsts c, DevScalars *ds,
                                                    double *__restrict__ phys, const cx<T> *__restrict__ tw) {
     extern __shared__ __align__(16) unsigned char smraw[];
     constexpr int Q = L / E;
@@ -407,9 +427,9 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
     const bool ok = pen < npen;
     const long long base = (ok ? pen : 0) * g.Kz;
     cx<T> *smc = reinterpret_cast<cx<T> *>(smraw);
-    SmPencil<T, L> sm{smc + p * SmPencil<T, L>::PITCH};
+    SmPencil<T, L, E> sm{smc + p * SmPencil<T, L, E>::PITCH};
     constexpr int NREG = K3Reg<T, MODE>::N;
-    T *ph = reinterpret_cast<T *>(smc + P * SmPencil<T, L>::PITCH) + (long long)p * K3Reg<T, MODE>::NSM * L;
+    T *ph = reinterpret_cast<T *>(smc + P * SmPencil<T, L, E>::PITCH) + (long long)p * K3Reg<T, MODE>::NSM * L;
     const T sz = T(g.sz);
     cx<T> *const B0 = buf + base;
 #define F(i) (B0 + (long long)(i) * g.S2)
@@ -418,9 +438,9 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
     if constexpr (MODE == MODE_VEL) {
         cx<T> A[E], B[E];
         k3_load_pair<T, L, E>(A, F(0), false, F(1), false, g.Kz, sz, q, ok);
-        fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(A, sm, q, tw);
+        fft<T, L, E, true, SmPencil<T, L, E>, (32 % (L / E) == 0)>(A, sm, q, tw);
         k3_load_pair<T, L, E>(B, F(2), false, nullptr, false, g.Kz, sz, q, ok);
-        fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(B, sm, q, tw);
+        fft<T, L, E, true, SmPencil<T, L, E>, (32 % (L / E) == 0)>(B, sm, q, tw);
         double ss = 0.0;
 #pragma unroll
         for (int e = 0; e < E; e++) {
@@ -451,7 +471,7 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
         cx<T> A[E];
         const cx<T> *src[6] = {F(0), F(1), F(2), F(3), F(4), F(5)};
         if constexpr (STAGE) {
-            cx<T> *st = smc + P * SmPencil<T, L>::PITCH + (long long)p * 2 * NSP * g.Kz;
+            cx<T> *st = smc + P * SmPencil<T, L, E>::PITCH + (long long)p * 2 * NSP * g.Kz;
 #pragma unroll
             for (int gp = FIRST; gp < 3; gp++) {
 #pragma unroll
@@ -485,7 +505,7 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
                 else if (pi == FIRST + 2) { cp_async_wait<0>(); __syncthreads(); }
             }
             k3_load_pair<T, L, E>(A, src[pi], false, src[pi + 3], false, g.Kz, sz, q, ok);
-            fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(A, sm, q, tw);
+            fft<T, L, E, true, SmPencil<T, L, E>, (32 % (L / E) == 0)>(A, sm, q, tw);
             if (pi == 0) {
 #pragma unroll
                 for (int e = 0; e < E; e++) { rs[0][e] = A[e].x; rs[1][e] = A[e].y; }
@@ -529,7 +549,7 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
             const cx<T> *fa = pi < 3 ? F(3 + pi) : pi == 3 ? F(0) : F(2);
             const cx<T> *fb = pi < 3 ? F(6 + pi) : pi == 3 ? F(1) : nullptr;
             k3_load_pair<T, L, E>(A, fa, pi >= 3, fb, pi == 3, g.Kz, sz, q, ok);
-            fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(A, sm, q, tw);
+            fft<T, L, E, true, SmPencil<T, L, E>, (32 % (L / E) == 0)>(A, sm, q, tw);
             switch (pi) {
             case 0:
 #pragma unroll
@@ -639,7 +659,7 @@ __global__ void __launch_bounds__(P *(L / E)) k3_z(Geo g, cx<T> *__restrict__ bu
             const int fa = pi == 0 ? 0 : pi == 1 ? 2 : pi == 5 ? 1 : pi + 1;
             const int fb = pi == 0 ? 1 : pi == 1 ? 0 : pi == 5 ? 2 : pi + 4;
             k3_load_pair<T, L, E>(A, F(fa), pi == 5, F(fb), pi == 1 || pi == 5, g.Kz, sz, q, ok);
-            fft<T, L, E, true, SmPencil<T, L>, (32 % (L / E) == 0)>(A, sm, q, tw);
+            fft<T, L, E, true, SmPencil<T, L, E>, (32 % (L / E) == 0)>(A, sm, q, tw);
             switch (pi) {
             case 0:
 #pragma unroll

@@ -1018,19 +1018,19 @@ __global__ void k_fft1d_lines(double2 *data, int batch, int sign, const double2 
     const long long line = (long long)blockIdx.x * P + p;
     const bool ok = line < batch;
     cx<double> *d = reinterpret_cast<cx<double> *>(data) + (ok ? line : 0) * L;
-    SmPencil<double, L> sm{reinterpret_cast<cx<double> *>(smraw) + p * SmPencil<double, L>::PITCH};
+    SmPencil<double, L, E> sm{reinterpret_cast<cx<double> *>(smraw) + p * SmPencil<double, L, E>::PITCH};
     cx<double> r[E];
     if (sign < 0) {
 #pragma unroll
         for (int e = 0; e < E; e++) r[e] = ok ? d[in_row<L, E, false>(q, e)] : zero<double>();
-        fft<double, L, E, false, SmPencil<double, L>, (32 % (L / E) == 0)>(r, sm, q, (const cx<double> *)tw);
+        fft<double, L, E, false, SmPencil<double, L, E>, (32 % (L / E) == 0)>(r, sm, q, (const cx<double> *)tw);
         if (ok)
 #pragma unroll
             for (int e = 0; e < E; e++) d[out_row<L, E, false>(q, e)] = r[e];
     } else {
 #pragma unroll
         for (int e = 0; e < E; e++) r[e] = ok ? d[in_row<L, E, true>(q, e)] : zero<double>();
-        fft<double, L, E, true, SmPencil<double, L>, (32 % (L / E) == 0)>(r, sm, q, (const cx<double> *)tw);
+        fft<double, L, E, true, SmPencil<double, L, E>, (32 % (L / E) == 0)>(r, sm, q, (const cx<double> *)tw);
         if (ok)
 #pragma unroll
             for (int e = 0; e < E; e++) d[out_row<L, E, true>(q, e)] = r[e];
