@@ -245,13 +245,11 @@ template <typename T> struct Passes {
         const bool prof = h->prof_steps < h->prof_cap_steps;
 #define MARK(name) do { if (prof) prof_mark(h, slot++, name); } while (0)
         if (h->a.eps_forcing > 0.0) {
-            MARK("shell_sums");
-            int r = shell_sums(h);
-            if (r) return r;
-            MARK("eps_alpha");
-            spns::k_eps_alpha<<<1, 1, 0, h->st>>>(h->bins, h->a.eps_kmin, h->a.eps_kmax, h->a.eps_forcing, h->ds);
+            MARK("eps_band");
+            spns::k_eps_band<T><<<1, spns::EPS_BAND_THREADS, 0, h->st>>>(h->g, U(h, 0), U(h, 1), U(h, 2), Ulo(h, 0), Ulo(h, 1), Ulo(h, 2),
+                                                                      h->a.eps_kmin, h->a.eps_kmax, h->a.eps_forcing, h->ds);
             CKL();
-            nk += 2;
+            nk += 1;
         }
         const int mode = h->a.isLES ? spns::MODE_LES : h->a.nonlinear_form == 2 ? spns::MODE_ADV : spns::MODE_ROT;
 #define STEP_PASSES(MD)                                                                       \

@@ -1153,11 +1153,48 @@ static __global__ void k_totals(const double *Ek, const double *Om, int Kmax, De
 
 // Constant-power forcing coefficient alpha = eps/(2 E_f), E_f the energy of
 // shells [kmin,kmax] of the current state (src/HIT_LES.cpp:250-256).
-static __global__ void k_eps_alpha(const double *Ek, int kmin, int kmax, double eps, DevScalars *ds) {
-    double Ef = 0.0;
-    for (int K = kmin; K <= kmax; K++) Ef += Ek[K];
-    ds->alpha = Ef > 1e-30 ? eps / (2.0 * Ef) : 0.0;
+// Constant-power forcing amplitude (the disabled block of src/HIT_LES.cpp:243-278,
+// with eps as a parameter): alpha = eps / (2 Ef), Ef the energy of the
+// shells kmin..kmax of the state (the sum over those shells of the E(K) of k_shell_sums).
+// Only modes with |s m| <= kmax + 1 on every axis can round into those shells,
+// so one block visits that sub-box directly, in a fixed order with a fixed
+// reduction tree: alpha does not depend on timing.  EPS_BAND_THREADS threads.
+constexpr int EPS_BAND_THREADS = 256;
+template <typename T>
+__global__ void __launch_bounds__(EPS_BAND_THREADS) k_eps_band(Geo g, const cx<T> *__restrict__ u, const cx<T> *__restrict__ v,
+                                                               const cx<T> *__restrict__ w, const cx<T> *__restrict__ ulo,
+                                                               const cx<T> *__restrict__ vlo, const cx<T> *__restrict__ wlo,
+                                                               int kmin, int kmax, double eps, DevScalars *ds) {
+    __shared__ double red[EPS_BAND_THREADS];
+    const int mx = min(g.hx, (kmax + 1) / g.sx), my = min(g.hy, (kmax + 1) / g.sy), mz = min(g.hz, (kmax + 1) / g.sz);
+    const int nx = 2 * mx + 1, ny = 2 * my + 1, nz = mz + 1;
+    const int count = nx * ny * nz;
+    double acc = 0.0;
+    for (int c = threadIdx.x; c < count; c += EPS_BAND_THREADS) {
+        const int kz = c % nz, t = c / nz;
+        const int m1 = t % nx - mx, m2 = t / nx - my;
+        const int ix = m1 >= 0 ? m1 : m1 + g.Kx, iy = m2 >= 0 ? m2 : m2 + g.Ky;
+        const long long k1 = (long long)g.sx * m1, k2 = (long long)g.sy * m2, k3 = (long long)g.sz * kz;
+        const int K = (int)round(sqrt((double)(k1 * k1 + k2 * k2 + k3 * k3)));
+        if (K < kmin || K > kmax) continue;
+        const long long idx = ((long long)iy * g.Kx + ix) * g.Kz + kz;
+        const cx<double> a = load_state(u, ulo, idx), b = load_state(v, vlo, idx), cc = load_state(w, wlo, idx);
+        double e = 0.5 * (a.x * a.x + a.y * a.y + b.x * b.x + b.y * b.y + cc.x * cc.x + cc.y * cc.y);
+        if (kz != 0) e *= 2.0;
+        acc += e;
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = EPS_BAND_THREADS / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double Ef = red[0];
+        ds->alpha = Ef > 1e-30 ? eps / (2.0 * Ef) : 0.0;
+    }
 }
+
 
 // src/HIT_LES.cpp:417-419: FT[K] = sqrt(Forced_Ek[K]/Ek[K]).
 static __global__ void k_forcing_factors(const double *Ek, const double *Forced, int last_eff, double *FT) {
