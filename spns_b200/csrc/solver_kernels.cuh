@@ -396,28 +396,31 @@ __device__ __forceinline__ T &k3_slot(T (&rg)[NREG > 0 ? NREG : 1][E], T *ph, in
 // three pairs use them, so the loads of the second and third pairs overlap the
 // transforms of the first.  Dynamic shared memory then holds P*6*Kz extra
 // complex values after the exchange buffers.
-// Minimum resident blocks per SM of the z pass (the register budget ptxas
-// allocates to): single precision 4 blocks (128 registers) for the velocity and
-// rotational forms, 3 for the advective and LES forms; double precision 1.
-#ifndef SPNS_K3_MINB_ROT
-#define SPNS_K3_MINB_ROT 1
+// Register budget of the z pass, as registers per thread (0: none), turned into
+// the minimum resident blocks per SM of __launch_bounds__ for the block size
+// at hand: single precision 128 for the velocity and rotational forms (16 warps
+// per SM), 168 for the advective and LES forms (12 warps); double precision none.
+#ifndef SPNS_K3_REGS_ROT
+#define SPNS_K3_REGS_ROT 0
 #endif
-#ifndef SPNS_K3_MINB_ADV
-#define SPNS_K3_MINB_ADV 1
+#ifndef SPNS_K3_REGS_ADV
+#define SPNS_K3_REGS_ADV 0
 #endif
-#ifndef SPNS_F32_K3_MINB_ROT
-#define SPNS_F32_K3_MINB_ROT 4
+#ifndef SPNS_F32_K3_REGS_ROT
+#define SPNS_F32_K3_REGS_ROT 128
 #endif
-#ifndef SPNS_F32_K3_MINB_ADV
-#define SPNS_F32_K3_MINB_ADV 3
+#ifndef SPNS_F32_K3_REGS_ADV
+#define SPNS_F32_K3_REGS_ADV 168
 #endif
-template <typename T, int MODE> struct K3MinBlocks {
+template <typename T, int MODE, int THREADS> struct K3MinBlocks {
     static constexpr bool D = sizeof(T) == 8;
-    static constexpr int N = (MODE == MODE_LES || MODE == MODE_ADV) ? (D ? SPNS_K3_MINB_ADV : SPNS_F32_K3_MINB_ADV)
-                           : (MODE == MODE_ROT || MODE == MODE_VEL) ? (D ? SPNS_K3_MINB_ROT : SPNS_F32_K3_MINB_ROT) : 1;
+    static constexpr int REGS = (MODE == MODE_LES || MODE == MODE_ADV) ? (D ? SPNS_K3_REGS_ADV : SPNS_F32_K3_REGS_ADV)
+                              : (MODE == MODE_ROT || MODE == MODE_VEL) ? (D ? SPNS_K3_REGS_ROT : SPNS_F32_K3_REGS_ROT) : 0;
+    static constexpr int B = REGS > 0 ? 65536 / (REGS * THREADS) : 1;
+    static constexpr int N = B < 1 ? 1 : B;
 };
 template <typename T, int L, int E, int P, int MODE, bool STAGE = false>
-__global__ void __launch_bounds__(P *(L / E), K3MinBlocks<T, MODE>::N) k3_z(Geo g, cx<T> *__restrict__ buf, StepConsts c, DevScalars *ds,
+__global__ void __launch_bounds__(P *(L / E), K3MinBlocks<T, MODE, P *(L / E)>::N) k3_z(Geo g, cx<T> *__restrict__ buf, StepConsts c, DevScalars *ds,
                                                    double *__restrict__ phys, const cx<T> *__restrict__ tw) {
     extern __shared__ __align__(16) unsigned char smraw[];
     constexpr int Q = L / E;
