@@ -209,7 +209,8 @@ def _timed_steps(h, n: int) -> float:
 
 
 def ensemble_block(local: int, n_boxes: int = 64, steps: int = 500, seed: int = 7):
-    """64 LES boxes of uneven size advanced together (one CUDA graph per step, FP32 form).
+    """64 LES boxes of uneven size advanced together (one CUDA graph per step, FP32 form,
+    launch shapes per box class picked by the autotuner).
 
     Grids uniform in {32,48,64,96}^3 (FFT 48..144), Cs uniform in [0.10, 0.20],
     nu=1e-4, per-instance Philox seeds with k_p=3, u_rms=1, CFL dt (C_At=0.5).
@@ -222,10 +223,11 @@ def ensemble_block(local: int, n_boxes: int = 64, steps: int = 500, seed: int = 
     rng = np.random.default_rng(seed)
     specs = [(int(rng.choice([32, 48, 64, 96])), float(rng.uniform(0.10, 0.20)), int(rng.integers(0, 2 ** 63)))
              for _ in range(n_boxes)]
-    members = []
+    members, shapes = [], {}
     for N, cs, sd in specs:
         h = HIT(sbox(N, nu=1e-4, C_Smag=cs), precision=SPNS_FP32_HILO, device=local)
         h.seed_field(sd, 3.0, 1.0)
+        shapes[str(N)] = h.autotune(steps=3)      # timed once per box class, then cached
         members.append(h)
     ens = Ensemble(members)
     ens.step(3)                                   # first step uncaptured, then graph capture
@@ -254,8 +256,11 @@ def ensemble_block(local: int, n_boxes: int = 64, steps: int = 500, seed: int = 
             "sequential_plain_fp64_box_steps_per_s": box_steps / seq["fp64"],
             "speedup_vs_sequential_fp32": seq["fp32_hilo"] / t_ens,
             "speedup_vs_sequential_plain_fp64": seq["fp64"] / t_ens,
-            "how": "one CUDA graph per step with every box's step as a parallel branch; sequential baselines "
-                   f"timed over {probe} steps per box and scaled to {steps}"}
+            "autotuned_shapes": {k: {"K1..K5 alternate (E=6)": v} for k, v in sorted(shapes.items(), key=lambda kv: int(kv[0]))},
+            "how": "one CUDA graph per step with every box's step as a parallel branch; launch shapes per box "
+                   "class picked by spns_autotune (the sequential FP32 baseline uses the same tuned shapes, the "
+                   f"plain FP64 one the defaults); sequential baselines timed over {probe} steps per box and "
+                   f"scaled to {steps}"}
 
 
 def serving_block(local: int, n_requests: int = 40, rate: float = 20.0, seed: int = 11, budget_gb: float = 150.0):

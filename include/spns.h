@@ -191,6 +191,23 @@ const char *spns_ensemble_last_error(spns_ensemble *e);
 
 /* Per-kernel CUDA-event profile of the next max_steps calls of one step
  * (events recorded on the handle's stream between the kernels of a step). */
+/* Autotuner of the launch shapes (FFT radix plan and tile per pass).  For each
+ * of the passes K1..K5 whose length has an alternate compiled shape (E = 6
+ * values per thread for lengths <= 192 in the step forms), times the default
+ * and the alternate over `steps` real steps of this handle (per-kernel CUDA
+ * events), keeps the faster per pass and restores the state it found, so the
+ * run is unchanged.  Choices are cached per process by precision, form and box;
+ * a later call or a handle created later for the same key uses them without
+ * timing.  `choice` (5 ints, or NULL) receives 0 (default) / 1 (alternate) for
+ * K1..K5.  Call it before an ensemble that holds the handle is stepped.
+ * It stands where the reference measures its FFT plans (FFTW_MEASURE,
+ * src/FFTW_package.h:12, at plan creation src/FFTW_package.cpp:53-55). */
+int spns_autotune(spns_handle *h, int steps, int *choice);
+/* Forgets the process-wide tuning cache (handles keep their shapes). */
+int spns_autotune_forget(void);
+/* Sets the shapes of K1..K5 directly (0 default, 1 alternate where compiled). */
+int spns_set_shapes(spns_handle *h, const int *choice);
+
 int spns_profile_begin(spns_handle *h, int max_steps);
 /* ms[s*nkernels + k] = duration of kernel k in profiled step s (synchronises). */
 int spns_profile_read(spns_handle *h, float *ms, int cap, int *nkernels, int *nsteps);

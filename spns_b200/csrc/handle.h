@@ -4,6 +4,8 @@
 #pragma once
 #include "spns.h"
 #include "solver_kernels.cuh"
+
+#include <type_traits>
 #include "edge_kernels.cuh"
 
 #include <cuda_runtime.h>
@@ -96,15 +98,29 @@ template <typename T, int L> using ShapeK1 = ShapeT<T, L, ShapeSel<T>::K1_E, Sha
 template <typename T, int L> using ShapeK2 = ShapeT<T, L, ShapeSel<T>::K2_E, ShapeSel<T>::K2_T>;   // inverse y (and forward y)
 template <typename T, int L> using ShapeK5 = ShapeT<T, L, ShapeSel<T>::K5_E, ShapeSel<T>::K5_T>;   // forward x
 template <typename T, int L> using Shape = ShapeT<T, L, 24, 128>;                                   // edge planes, test lines
+// Alternate shapes the autotuner (spns_autotune) can pick per pass for short
+// lengths: E = 6 values per thread (radix plan 6 x 2 x ... or 6 x 6 x ...),
+// four times the threads per pencil of the default E = 24, which small boxes
+// need to fill the GPU.  Compiled for the step forms at L <= SPNS_ALT_MAX_L.
+#ifndef SPNS_ALT_MAX_L
+#define SPNS_ALT_MAX_L 192
+#endif
+constexpr int SPNS_ALT_E = 6;
+template <int L, int MODE> constexpr bool shape_alt_ok() {
+    return L <= SPNS_ALT_MAX_L && (MODE == spns::MODE_ROT || MODE == spns::MODE_ADV || MODE == spns::MODE_LES);
+}
+template <typename T, int L, int ALT> using ShapeK1A = typename std::conditional<ALT != 0, ShapeT<T, L, SPNS_ALT_E, ShapeSel<T>::K1_T>, ShapeK1<T, L>>::type;
+template <typename T, int L, int ALT> using ShapeK2A = typename std::conditional<ALT != 0, ShapeT<T, L, SPNS_ALT_E, ShapeSel<T>::K2_T>, ShapeK2<T, L>>::type;
+template <typename T, int L, int ALT> using ShapeK5A = typename std::conditional<ALT != 0, ShapeT<T, L, SPNS_ALT_E, ShapeSel<T>::K5_T>, ShapeK5<T, L>>::type;
 
 // z pass: pencils per block limited by the shared memory of the exchange
 // buffer plus the physical fields kept per pencil.
-template <typename T, int L, int MODE> struct Shape3 {
-    static constexpr int E = (MODE == spns::MODE_ROT || MODE == spns::MODE_VEL) ? ShapeSel<T>::Z_E_ROT : ShapeSel<T>::Z_E;
+template <typename T, int L, int MODE, int ALT = 0> struct Shape3 {
+    static constexpr int E = ALT ? SPNS_ALT_E : (MODE == spns::MODE_ROT || MODE == spns::MODE_VEL) ? ShapeSel<T>::Z_E_ROT : ShapeSel<T>::Z_E;
     static constexpr int Q = L / E;
     static constexpr int ZT = ShapeSel<T>::Z_T / Q;
     static constexpr int P0 = ZT >= 32 ? 32 : ZT >= 16 ? 16 : ZT >= 8 ? 8 : ZT >= 4 ? 4 : ZT >= 2 ? 2 : 1;
-    static constexpr size_t PER_PEN = (size_t)spns::SmPencil<T, L, E>::PITCH * sizeof(spns::cx<T>) + (size_t)spns::K3Reg<T, MODE>::NSM * L * sizeof(T);
+    static constexpr size_t PER_PEN = (size_t)spns::SmPencil<T, L, E>::PITCH * sizeof(spns::cx<T>) + (size_t)spns::K3Reg<T, MODE, E>::NSM * L * sizeof(T);
     static constexpr int PMAX = (int)((200 * 1024) / PER_PEN);
     static constexpr int P = P0 <= PMAX ? P0 : PMAX >= 16 ? 16 : PMAX >= 8 ? 8 : PMAX >= 4 ? 4 : PMAX >= 2 ? 2 : 1;
     static constexpr int THREADS = P * Q;
@@ -146,6 +162,9 @@ struct spns_handle {
     int edge_launches = 0;                           // launches of the edge correction in the last step
     // CUDA graphs of one step, per parity of the state-buffer swap (kappa scheme)
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    // launch shape per pass (index 1..5 = K1..K5): 0 default, 1 the alternate of
+    // shape_alt_ok lengths; set by spns_autotune or from its per-process cache
+    unsigned char shape_alt[6] = {0, 0, 0, 0, 0, 0};
     void *U0 = nullptr;                              // state buffer of parity 0
     bool use_graphs = true;
     // optional per-kernel event profile of the next steps (spns_profile_*)

@@ -15,8 +15,8 @@ template <typename T> struct Passes {
     static C *Ulo(spns_handle *h, int f = 0) { return HILO ? (C *)h->Ulo + (long long)f * h->g.S0 : nullptr; }
     static const C *tw(spns_handle *h, int L) { return (const C *)h->tw[L]; }
 
-    template <int L, int MODE> static cudaError_t launch_k1(spns_handle *h) {
-        using S = ShapeK1<T, L>;
+    template <int L, int MODE, int ALT = 0> static cudaError_t launch_k1(spns_handle *h) {
+        using S = ShapeK1A<T, L, ALT>;
         auto kern = spns::k1_inv_x<T, L, S::E, S::P, MODE>;
         cudaError_t e = spns_set_smem(kern, S::SMEM_ROW);
         if (e != cudaSuccess) return e;
@@ -24,8 +24,8 @@ template <typename T> struct Passes {
         kern<<<grid, S::THREADS, S::SMEM_ROW, h->st>>>(h->g, U(h, 0), U(h, 1), U(h, 2), (C *)h->B1, tw(h, L));
         return cudaGetLastError();
     }
-    template <int L, int MODE> static cudaError_t launch_k2(spns_handle *h) {
-        using S = ShapeK2<T, L>;
+    template <int L, int MODE, int ALT = 0> static cudaError_t launch_k2(spns_handle *h) {
+        using S = ShapeK2A<T, L, ALT>;
         auto kern = spns::k2_inv_y<T, L, S::E, S::P, MODE>;
         cudaError_t e = spns_set_smem(kern, S::SMEM_ROW);
         if (e != cudaSuccess) return e;
@@ -33,8 +33,8 @@ template <typename T> struct Passes {
         kern<<<grid, S::THREADS, S::SMEM_ROW, h->st>>>(h->g, (const C *)h->B1, (C *)h->B2, tw(h, L));
         return cudaGetLastError();
     }
-    template <int L, int MODE> static cudaError_t launch_k3(spns_handle *h, double *phys) {
-        using S3 = Shape3<T, L, MODE>;
+    template <int L, int MODE, int ALT = 0> static cudaError_t launch_k3(spns_handle *h, double *phys) {
+        using S3 = Shape3<T, L, MODE, ALT>;
         constexpr bool STAGE = MODE == spns::MODE_ROT && ShapeSel<T>::Z_STAGE;
         auto kern = spns::k3_z<T, L, S3::E, S3::P, MODE, STAGE>;
         const size_t smem = S3::SMEM + (STAGE ? (size_t)S3::P * 2 * spns::K3StagePairs<T>::N * h->g.Kz * sizeof(C) : 0);
@@ -45,8 +45,8 @@ template <typename T> struct Passes {
         kern<<<grid, S3::THREADS, smem, h->st>>>(h->g, (C *)h->B2, h->c, h->ds, phys, tw(h, L));
         return cudaGetLastError();
     }
-    template <int L, int MODE> static cudaError_t launch_k4(spns_handle *h) {
-        using S = ShapeK2<T, L>;
+    template <int L, int MODE, int ALT = 0> static cudaError_t launch_k4(spns_handle *h) {
+        using S = ShapeK2A<T, L, ALT>;
         auto kern = spns::k4_fwd_y<T, L, S::E, S::P, MODE>;
         cudaError_t e = spns_set_smem(kern, S::SMEM_ROW);
         if (e != cudaSuccess) return e;
@@ -54,8 +54,8 @@ template <typename T> struct Passes {
         kern<<<grid, S::THREADS, S::SMEM_ROW, h->st>>>(h->g, (const C *)h->B2, (C *)h->B1, tw(h, L));
         return cudaGetLastError();
     }
-    template <int L, int MODE> static cudaError_t launch_k5(spns_handle *h) {
-        using S = ShapeK5<T, L>;
+    template <int L, int MODE, int ALT = 0> static cudaError_t launch_k5(spns_handle *h) {
+        using S = ShapeK5A<T, L, ALT>;
         auto kern = spns::k5_fwd_x<T, L, S::E, S::P, MODE>;
         cudaError_t e = spns_set_smem(kern, S::SMEM_ROW);
         if (e != cudaSuccess) return e;
@@ -63,6 +63,20 @@ template <typename T> struct Passes {
         kern<<<grid, S::THREADS, S::SMEM_ROW, h->st>>>(h->g, (const C *)h->B1, (C *)h->B2, tw(h, L));
         return cudaGetLastError();
     }
+    // Launch of pass K1..K5 in the shape the handle selected (shape_alt).
+#define SPNS_SELECT(name, idx, ...)                                                              \
+    template <int L, int MODE> static cudaError_t sel_##name(spns_handle *h) {                    \
+        if constexpr (shape_alt_ok<L, MODE>())                                                    \
+            if (h->shape_alt[idx]) return launch_##name<L, MODE, 1>(h __VA_ARGS__);               \
+        return launch_##name<L, MODE, 0>(h __VA_ARGS__);                                          \
+    }
+    SPNS_SELECT(k1, 1)
+    SPNS_SELECT(k2, 2)
+    SPNS_SELECT(k3, 3, , nullptr)
+    SPNS_SELECT(k4, 4)
+    SPNS_SELECT(k5, 5)
+#undef SPNS_SELECT
+
     // Spectral sweep; with the kappa scheme the new state goes into the u^{n-1}
     // buffers and the state buffers are swapped after the launch.
     static cudaError_t launch_k6(spns_handle *h) {
@@ -254,18 +268,18 @@ template <typename T> struct Passes {
         const int mode = h->a.isLES ? spns::MODE_LES : h->a.nonlinear_form == 2 ? spns::MODE_ADV : spns::MODE_ROT;
 #define STEP_PASSES(MD)                                                                       \
         MARK("k1_inv_x");                                                                     \
-        DISPATCH(h->g.Mx, LAUNCH((launch_k1<LL, MD>(h))));                                    \
+        DISPATCH(h->g.Mx, LAUNCH((sel_k1<LL, MD>(h))));                                    \
         MARK("k2_inv_y");                                                                     \
-        DISPATCH(h->g.My, LAUNCH((launch_k2<LL, MD>(h))));                                    \
+        DISPATCH(h->g.My, LAUNCH((sel_k2<LL, MD>(h))));                                    \
         MARK("reset_max");                                                                    \
         spns::k_reset_max<<<1, 1, 0, h->st>>>(h->ds);                                         \
         CKL();                                                                                \
         MARK("k3_z");                                                                         \
-        DISPATCH(h->g.Mz, LAUNCH((launch_k3<LL, MD>(h, nullptr))));                           \
+        DISPATCH(h->g.Mz, LAUNCH((sel_k3<LL, MD>(h))));                           \
         MARK("k4_fwd_y");                                                                     \
-        DISPATCH(h->g.My, LAUNCH((launch_k4<LL, MD>(h))));                                    \
+        DISPATCH(h->g.My, LAUNCH((sel_k4<LL, MD>(h))));                                    \
         MARK("k5_fwd_x");                                                                     \
-        DISPATCH(h->g.Mx, LAUNCH((launch_k5<LL, MD>(h))));                                    \
+        DISPATCH(h->g.Mx, LAUNCH((sel_k5<LL, MD>(h))));                                    \
         if (MD == spns::MODE_ROT && h->edge) {                                                \
             MARK("edge_correction");                                                          \
             int r_ = edge_correction(h);                                                      \

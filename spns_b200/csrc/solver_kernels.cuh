@@ -380,8 +380,9 @@ template <int MODE> struct K3Phys { static constexpr int N = MODE == MODE_ADV ? 
 #define SPNS_F32_Z_STAGE_PAIRS 3
 #endif
 template <typename T> struct K3StagePairs { static constexpr int N = sizeof(T) == 8 ? SPNS_Z_STAGE_PAIRS : SPNS_F32_Z_STAGE_PAIRS; };
-template <typename T, int MODE> struct K3Reg {
-    static constexpr int R = sizeof(T) == 8 ? SPNS_K3_REG_SLOTS : SPNS_F32_K3_REG_SLOTS;
+template <typename T, int MODE, int E = 12> struct K3Reg {
+    // with few values per thread (E <= 6) more slots fit in registers
+    static constexpr int R = E <= 6 ? (sizeof(T) == 8 ? 8 : 12) : sizeof(T) == 8 ? SPNS_K3_REG_SLOTS : SPNS_F32_K3_REG_SLOTS;
     static constexpr int N = K3Phys<MODE>::N < R ? K3Phys<MODE>::N : R;   // slots in registers
     static constexpr int NSM = K3Phys<MODE>::N - N;                       // slots in shared memory
 };
@@ -431,8 +432,8 @@ __global__ void __launch_bounds__(P *(L / E), K3MinBlocks<T, MODE, P *(L / E)>::
     const long long base = (ok ? pen : 0) * g.Kz;
     cx<T> *smc = reinterpret_cast<cx<T> *>(smraw);
     SmPencil<T, L, E> sm{smc + p * SmPencil<T, L, E>::PITCH};
-    constexpr int NREG = K3Reg<T, MODE>::N;
-    T *ph = reinterpret_cast<T *>(smc + P * SmPencil<T, L, E>::PITCH) + (long long)p * K3Reg<T, MODE>::NSM * L;
+    constexpr int NREG = K3Reg<T, MODE, E>::N;
+    T *ph = reinterpret_cast<T *>(smc + P * SmPencil<T, L, E>::PITCH) + (long long)p * K3Reg<T, MODE, E>::NSM * L;
     const T sz = T(g.sz);
     cx<T> *const B0 = buf + base;
 #define F(i) (B0 + (long long)(i) * g.S2)

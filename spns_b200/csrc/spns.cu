@@ -9,7 +9,11 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
+#include <array>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 using namespace spns;
 
@@ -352,6 +356,8 @@ const char *spns_status_string(int s) {
 
 const char *spns_last_error(spns_handle *h) { return h ? h->err.c_str() : g_create_error.c_str(); }
 
+static void apply_cached_shapes(spns_handle *h);
+
 int spns_create(const spns_hit_args *args, const double *file_uvw, spns_handle **out) {
     spns_handle *h = nullptr;
     if (!args || !out) return spns_fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "null argument");
@@ -469,6 +475,7 @@ int spns_create(const spns_hit_args *args, const double *file_uvw, spns_handle *
     rc = read_scalars(h, &sv);
     if (rc) { g_create_error = h->err; return cleanup(rc); }
     h->Ek_init = sv.ek_tot;
+    apply_cached_shapes(h);
     *out = h;
     return SPNS_OK;
 }
@@ -709,6 +716,122 @@ int spns_profile_read(spns_handle *h, float *ms, int cap, int *nkernels, int *ns
         }
     (void)per;
     h->prof_cap_steps = 0;
+    return SPNS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner of the launch shapes: per pass K1..K5, the default shape or the
+// alternate (E = 6 values per thread: another radix plan and four times the
+// threads per pencil) where one is compiled (short lengths, step forms).  Both
+// are timed on the handle's own box with per-kernel CUDA events over real
+// steps; the state is saved before and restored after, so tuning leaves the run
+// unchanged.  Choices are cached per process by precision, form and box, and
+// handles created later for the same key take them without tuning.
+// ---------------------------------------------------------------------------
+namespace {
+using TuneKey = std::tuple<int, int, int, int, int, int, int, int>;
+std::mutex g_tune_mu;
+std::map<TuneKey, std::array<unsigned char, 6>> g_tune_cache;
+TuneKey tune_key(const spns_handle *h) {
+    const int mode = h->a.isLES ? MODE_LES : h->a.nonlinear_form == 2 ? MODE_ADV : MODE_ROT;
+    return TuneKey(h->prec, mode, h->g.Mx, h->g.My, h->g.Mz, h->g.Kx, h->g.Ky, h->g.Kz);
+}
+// passes that have an alternate shape for this box
+void alt_passes(const spns_handle *h, bool has[6]) {
+    const int lim = SPNS_ALT_MAX_L;
+    has[0] = false;
+    has[1] = has[5] = h->g.Mx <= lim;
+    has[2] = has[4] = h->g.My <= lim;
+    has[3] = h->g.Mz <= lim;
+}
+void set_shapes(spns_handle *h, const std::array<unsigned char, 6> &sel) {
+    bool changed = false;
+    for (int i = 0; i < 6; i++) { changed = changed || h->shape_alt[i] != sel[i]; h->shape_alt[i] = sel[i]; }
+    if (!changed) return;
+    // captured steps hold the old kernels; the next step runs uncaptured (it sets
+    // the new kernels' attributes) and recaptures
+    for (auto &gx : h->graph) if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
+    h->kernels_per_step = 0;
+}
+} // namespace
+
+static void apply_cached_shapes(spns_handle *h) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(tune_key(h));
+    if (it != g_tune_cache.end()) set_shapes(h, it->second);
+}
+
+int spns_autotune(spns_handle *h, int steps, int *choice) {
+    if (!h || steps < 1 || steps > 64) return SPNS_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(h->a.device));
+    const TuneKey key = tune_key(h);
+    std::array<unsigned char, 6> best = {0, 0, 0, 0, 0, 0};
+    bool cached = false;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) { best = it->second; cached = true; }
+    }
+    bool has[6];
+    alt_passes(h, has);
+    bool any = false;
+    for (int i = 1; i <= 5; i++) any = any || has[i];
+    if (!cached && any) {
+        int r = check_flags(h);
+        if (r) return r;
+        size_t nb = 0;
+        r = spns_checkpoint_bytes(h, &nb);
+        if (r) return r;
+        std::vector<unsigned char> blob(nb);
+        r = spns_checkpoint_save(h, blob.data(), nb);
+        if (r) return r;
+        static const char *names[6] = {"", "k1_inv_x", "k2_inv_y", "k3_z", "k4_fwd_y", "k5_fwd_x"};
+        double t[2][6] = {};
+        std::vector<float> ms((size_t)steps * 16);
+        for (int cand = 0; cand < 2 && r == SPNS_OK; cand++) {
+            std::array<unsigned char, 6> sel = {0, 0, 0, 0, 0, 0};
+            for (int i = 1; i <= 5; i++) sel[i] = (unsigned char)(has[i] ? cand : 0);
+            set_shapes(h, sel);
+            r = spns_step_async(h, 1);                  // uncaptured: sets the kernels' attributes
+            if (!r) r = spns_profile_begin(h, steps);
+            if (!r) r = spns_step_async(h, steps);
+            int nk = 0, ns = 0;
+            if (!r) r = spns_profile_read(h, ms.data(), (int)ms.size(), &nk, &ns);
+            for (int k = 0; k < nk && !r; k++)
+                for (int i = 1; i <= 5; i++)
+                    if (h->prof_names[k] == names[i])
+                        for (int sidx = 0; sidx < ns; sidx++) t[cand][i] += ms[(size_t)sidx * nk + k];
+        }
+        const int rl = spns_checkpoint_load(h, blob.data(), nb);   // restore whatever happened
+        if (r) return r;
+        if (rl) return rl;
+        for (int i = 1; i <= 5; i++) best[i] = (unsigned char)(has[i] && t[1][i] < t[0][i] ? 1 : 0);
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_cache[key] = best;
+    }
+    set_shapes(h, best);
+    if (choice)
+        for (int i = 0; i < 5; i++) choice[i] = best[i + 1];
+    return SPNS_OK;
+}
+
+int spns_autotune_forget(void) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache.clear();
+    return SPNS_OK;
+}
+
+int spns_set_shapes(spns_handle *h, const int *choice) {
+    if (!h || !choice) return SPNS_ERR_INVALID_ARGUMENT;
+    bool has[6];
+    alt_passes(h, has);
+    std::array<unsigned char, 6> sel = {0, 0, 0, 0, 0, 0};
+    for (int i = 1; i <= 5; i++) {
+        if (choice[i - 1] < 0 || choice[i - 1] > 1) return spns_fail(h, SPNS_ERR_INVALID_ARGUMENT, "shape choice must be 0 or 1");
+        if (choice[i - 1] && !has[i]) return spns_fail(h, SPNS_ERR_INVALID_ARGUMENT, "pass K%d has no alternate shape for this box", i);
+        sel[i] = (unsigned char)choice[i - 1];
+    }
+    set_shapes(h, sel);
     return SPNS_OK;
 }
 

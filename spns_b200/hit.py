@@ -33,8 +33,13 @@ EXPORTED_SYMBOLS = (
     "spns_energy_cascade_noalloc_f64", "spns_estimate_device_bytes", "spns_seed_field", "spns_step_async",
     "spns_query", "spns_synchronize", "spns_checkpoint_bytes", "spns_checkpoint_save", "spns_checkpoint_load",
     "spns_ensemble_create", "spns_ensemble_step", "spns_ensemble_destroy", "spns_ensemble_last_error",
-    "spns_invariant_spectra",
+    "spns_invariant_spectra", "spns_autotune", "spns_autotune_forget", "spns_set_shapes",
 )
+
+
+def autotune_forget():
+    """Clears the process-wide cache of tuned launch shapes."""
+    lib().spns_autotune_forget()
 
 
 class SpnsError(RuntimeError):
@@ -132,6 +137,9 @@ def lib():
         L.spns_ensemble_last_error.argtypes = [vp]
         L.spns_ensemble_last_error.restype = C.c_char_p
         L.spns_invariant_spectra.argtypes = [vp, dp]
+        L.spns_autotune.argtypes = [vp, i, ip]
+        L.spns_autotune_forget.argtypes = []
+        L.spns_set_shapes.argtypes = [vp, ip]
         _lib = L
     return _lib
 
@@ -343,6 +351,19 @@ class HIT:
         n = C.c_int()
         self._ck(self._L.spns_kernels_per_step(self._h, C.byref(n)))
         return n.value
+
+    # --- launch-shape autotuner ---
+    def autotune(self, steps: int = 3):
+        """Times the default and the alternate launch shape of each pass on this box
+        (spns_autotune) and keeps the faster; the state is left as it was.  Returns
+        the choice per pass K1..K5 (0 default, 1 alternate)."""
+        ch = (C.c_int * 5)()
+        self._ck(self._L.spns_autotune(self._h, int(steps), ch))
+        return list(ch)
+
+    def set_shapes(self, choice):
+        ch = (C.c_int * 5)(*[int(x) for x in choice])
+        self._ck(self._L.spns_set_shapes(self._h, ch))
 
     def profile_begin(self, max_steps: int):
         self._ck(self._L.spns_profile_begin(self._h, int(max_steps)))

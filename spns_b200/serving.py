@@ -70,8 +70,9 @@ class SolveResult:
 class GpuBackend:
     """libspns handles: one per admitted run."""
 
-    def __init__(self, device: int = 0):
+    def __init__(self, device: int = 0, autotune: bool = True):
         self.device = device
+        self.autotune = autotune
 
     def device_bytes(self, req: SolveRequest) -> int:
         from .hit import estimate_device_bytes
@@ -84,6 +85,8 @@ class GpuBackend:
             h.checkpoint_load(req.init)
         else:
             h.seed_field(req.seed, req.kp, req.urms)
+        if self.autotune:
+            h.autotune(steps=2)       # timed on the first run of a box class, cached after
         return h
 
     def step_async(self, inst, n: int):
