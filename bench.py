@@ -55,7 +55,7 @@ def box_args(N: int, self_adaptive: bool = True, nxy: int = 0, shape=None):
                    isRotating=False, isLES=False, isComplexConjugateCorrected=False, isSelfAdaptive=self_adaptive)
 
 
-def algorithmic_bytes(N: int, self_adaptive: bool = True, word: int = 16, form: str = "rotational"):
+def algorithmic_bytes(N: int, self_adaptive: bool = True, word: int = 16, form: str = "rotational", shape=None):
     """Bytes each kernel must move once (arrays read + written, each counted once).
 
     S0 = compact spectral field, S1 = after the x transform, S2 = after the y
@@ -64,9 +64,10 @@ def algorithmic_bytes(N: int, self_adaptive: bool = True, word: int = 16, form: 
     advective form: 3 S0 -> 6 S1, 6 S1 -> 9 S2, 9 S2 -> 3 S2.  Then K4 3 S2 -> 3 S1,
     K5 3 S1 -> 3 S0 (nonlinear term G), K6 reads G, u, R^{n-1} (+ u^{n-1}) and writes
     R^n, u^{n+1}.  The edge correction moves O(M^2) bytes (negligible)."""
-    h = N // 2
-    K, M, Kz = 2 * h + 1, (3 * N) // 2, h + 1
-    S0, S1, S2 = K * K * Kz, K * M * Kz, M * M * Kz
+    Nx, Ny, Nz = shape or (N, N, N)
+    Kx, Ky, Kz = 2 * (Nx // 2) + 1, 2 * (Ny // 2) + 1, Nz // 2 + 1
+    Mx, My = (3 * Nx) // 2, (3 * Ny) // 2
+    S0, S1, S2 = Ky * Kx * Kz, Ky * Mx * Kz, My * Mx * Kz
     n1, n2 = (6, 9) if form == "advective" else (5, 6)
     return {
         "k1_inv_x": (3 * S0 + n1 * S1) * word,
@@ -433,7 +434,7 @@ def run_gpu(args):
     value = whole_job_rate(world, args.steps, ms_max / 1e3)
     e2e_value = whole_job_rate(world, args.steps, e2e_max)
     # roofline of the dominant kernel
-    bytes_per, sizes = algorithmic_bytes(N)
+    bytes_per, sizes = algorithmic_bytes(N, shape=(a.Nx, a.Ny, a.Nz))
     mean_ms = per.mean(axis=0)
     share = {n: float(m) for n, m in zip(names, mean_ms)}
     dom = max((n for n in names if n in bytes_per), key=lambda n: share[n])
