@@ -264,6 +264,45 @@ def ensemble_block(local: int, n_boxes: int = 64, steps: int = 500, seed: int = 
                    f"scaled to {steps}"}
 
 
+def les_config_block(local: int, steps: int = 2000):
+    """The LES configuration: rotating Smagorinsky LES (C_s=0.17, Omega=(0,0,1), nu=1e-4)
+    on the non-cubic box Nx=Ny=128, Nz=256 with Lz=2 (FFT grid 192 x 192 x 384), seeded
+    k_p=3 field with u_rms=1, CFL time step, `steps` steps in the compensated FP32 form
+    and in the FP64 form; E(K), total energy and eddy-viscosity statistics of FP32
+    against FP64 at the end."""
+    import numpy as np
+    from spns_b200.hit import HIT, SPNS_FP64, SPNS_FP32_HILO
+    from spns_b200.params import HitArgs
+    ex = lambda n, f: n * f  # noqa: E731  (even sizes)
+    a = HitArgs(Nx=128, Ny=128, Nz=ex(128, 2), Mx=192, My=192, Mz=ex(192, 2), nu=1e-4, C_Smag=0.17, C_At=C_AT,
+                Lx=1, Ly=1, Lz=2, omega_x=0.0, omega_y=0.0, omega_z=1.0, Nx_file=-1, Ny_file=-1, Nz_file=-1,
+                isReLambda=False, isInitialFieldFromBinaryFile=False, isInitialFieldFromASCIIFile=False,
+                isNotCubic=True, isRotating=True, isLES=True, isComplexConjugateCorrected=False, isSelfAdaptive=False)
+    runs, rate, probe = {}, {}, 50
+    for prec in (SPNS_FP64, SPNS_FP32_HILO):
+        h = HIT(a, precision=prec, device=local)
+        h.seed_field(3, 3.0, 1.0)
+        h.New_Fractional_Step_Method(3)
+        rate[prec] = probe / _timed_steps(h, probe)
+        h.New_Fractional_Step_Method(steps - 3 - probe)
+        runs[prec] = h
+    e64, e32 = runs[SPNS_FP64].Recalculate_Energy_Cascade(), runs[SPNS_FP32_HILO].Recalculate_Energy_Cascade()
+    m = e64 > 1e-6 * e64.max()
+    n64, n32 = runs[SPNS_FP64].eddy_viscosity_stats(), runs[SPNS_FP32_HILO].eddy_viscosity_stats()
+    rel = np.abs(n32 - n64) / n64
+    out = {"workload": "LES C_s=0.17, Omega=(0,0,1), Nx=Ny=128, Nz=256 (Lz=2; FFT 192x192x384), nu=1e-4, "
+                       f"seeded k_p=3, CFL dt, {steps} steps",
+           "fp32_hilo_steps_per_s": rate[SPNS_FP32_HILO], "fp64_steps_per_s": rate[SPNS_FP64],
+           "speedup_fp32_vs_fp64": rate[SPNS_FP32_HILO] / rate[SPNS_FP64],
+           "ek_max_shell_rel_err": float(np.max(np.abs(e32[m] - e64[m]) / e64[m])),
+           "etot_rel_err": float(abs(e32.sum() - e64.sum()) / e64.sum()),
+           "nu_t_fp64_mean_rms_max": n64.tolist(), "nu_t_rel_err_mean_rms_max": rel.tolist(),
+           "tolerances": {"ek_shell": 2e-5, "etot": 1e-6, "nu_t_mean_rms": 1e-6, "nu_t_max": 5e-5}}
+    for h in runs.values():
+        h.close()
+    return out
+
+
 def serving_block(local: int, n_requests: int = 40, rate: float = 20.0, seed: int = 11, budget_gb: float = 150.0):
     """Served workload: Poisson arrivals of LES/DNS runs, continuous batching.
 
@@ -473,6 +512,8 @@ def run_gpu(args):
                      "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                      "algorithmic_bytes": bytes_per[dom]},
     }
+    if not args.no_les:
+        line["les_config"] = les_config_block(local)
     if not args.no_ensemble:
         line["ensemble"] = ensemble_block(local)
     if not args.no_serving:
@@ -503,6 +544,7 @@ def main():
     ap.add_argument("--no-fp32", action="store_true", help="skip the compensated FP32 form's extra line field")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-box LES ensemble field")
     ap.add_argument("--no-serving", action="store_true", help="skip the served-workload field")
+    ap.add_argument("--no-les", action="store_true", help="skip the LES-configuration field (FP32 vs FP64)")
     ap.add_argument("--serving-requests", type=int, default=40)
     args = ap.parse_args()
     if args.warmup < 3:

@@ -120,6 +120,13 @@ int spns_check_physfour_energy(spns_handle *h, double atol, int *ok, double *dif
  * uses the gradients of the last step's start).  The first call allocates work
  * buffers of the advective step's size (6 S1 + 9 S2 fields), kept until destroy. */
 int spns_invariant_spectra(spns_handle *h, double *spectra);
+/* Eddy-viscosity statistics of the current state: stats[0] mean, stats[1] root
+ * mean square, stats[2] maximum over the grid of nu_t = (C_s Delta)^2
+ * sqrt(2 S_ij S_ij), the nu_t of Recalculate_Eddy_Viscosity
+ * (src/HIT_LES.cpp:130-142); zero for a DNS handle.  Runs the invariant passes
+ * (same work buffers as spns_invariant_spectra).  The reference writes no such
+ * statistics; they carry the FP32-against-FP64 comparison of an LES run. */
+int spns_eddy_viscosity_stats(spns_handle *h, double *stats);
 
 /* getters / HIT::setnu (src/HIT_LES.h:187-201) */
 int spns_get_scalars(spns_handle *h, spns_scalars *out);

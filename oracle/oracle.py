@@ -58,6 +58,7 @@ def lib():
             getattr(L, name).restype = d
         L.orc_recalculate_energy_cascade.argtypes = [vp, dp]
         L.orc_invariant_spectra.argtypes = [vp, dp]
+        L.orc_eddy_viscosity_stats.argtypes = [vp, dp]
         L.orc_recalculate_energy_cascade.restype = d
         L.orc_check_physfour_energy.argtypes = [vp, d, dp, dp]
         L.orc_check_physfour_energy.restype = i
@@ -143,6 +144,12 @@ class OracleHIT:
         s = self._scalars()
         out = np.zeros((5, int(s[12]) + 1))
         self._L.orc_invariant_spectra(self._h, _dp(out))
+        return out
+
+    def eddy_viscosity_stats(self):
+        """Mean, rms and maximum of nu_t over the grid (src/HIT_LES.cpp:130-142)."""
+        out = np.zeros(3)
+        self._L.orc_eddy_viscosity_stats(self._h, _dp(out))
         return out
 
     def Recalculate_Energy_Cascade(self):

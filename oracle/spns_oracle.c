@@ -532,6 +532,35 @@ void orc_invariant_spectra(orc *o, double *out) {
     free(fk);
 }
 
+/* Eddy-viscosity statistics over the grid: mean, root mean square and maximum of
+ * nu_t = (C_s Delta)^2 sqrt(2 S_ij S_ij) of the current state (the nu_t of
+ * Recalculate_Eddy_Viscosity, src/HIT_LES.cpp:130-142, same expression order). */
+void orc_eddy_viscosity_stats(orc *o, double *out) {
+    velocity_gradients(o);
+    cplx **gks[3] = {o->gradu_k, o->gradv_k, o->gradw_k};
+    double **gs[3] = {o->gradu, o->gradv, o->gradw};
+    for (int c = 0; c < 3; c++)
+        for (int d = 0; d < 3; d++) fft_c2r(o, gks[c][d], gs[c][d]);
+    const double ct = o->C_Smag * o->C_Smag * o->delta * o->delta;
+    double **gu = o->gradu, **gv = o->gradv, **gw = o->gradw;
+    double sum = 0.0, sq = 0.0, mx = 0.0;
+    long n = 0;
+    LOOP_REAL(o) {
+        long ind = IND_R(o);
+        double ne = 2.0 * gu[0][ind] * gu[0][ind];
+        ne += 2.0 * gv[1][ind] * gv[1][ind];
+        ne += 2.0 * gw[2][ind] * gw[2][ind];
+        ne += (gu[1][ind] + gv[0][ind]) * (gu[1][ind] + gv[0][ind]);
+        ne += (gu[2][ind] + gw[0][ind]) * (gu[2][ind] + gw[0][ind]);
+        ne += (gv[2][ind] + gw[1][ind]) * (gv[2][ind] + gw[1][ind]);
+        const double nt = ct * sqrt(ne);
+        sum += nt; sq += nt * nt; mx = nt > mx ? nt : mx; n++;
+    }
+    out[0] = sum / (double)n;
+    out[1] = sqrt(sq / (double)n);
+    out[2] = mx;
+}
+
 static void sgs_divergence(orc *o) { /* :130-192 */
     const double ct = o->C_Smag * o->C_Smag * o->delta * o->delta;
     double **gu = o->gradu, **gv = o->gradv, **gw = o->gradw;

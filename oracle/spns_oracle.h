@@ -63,6 +63,7 @@ double orc_recalculate_energy_cascade(orc *o, double *Ek_out); /* Ek_out[0..last
 /* Recalculate_Invariants_Distribution: spectra of Q_G, Q_S, R_G, R_S, V^2 of the
  * current state, out[c*(last_rad_max+1) + K]. */
 void orc_invariant_spectra(orc *o, double *out);
+void orc_eddy_viscosity_stats(orc *o, double *out);
 void orc_velocity_antitransform(orc *o);
 void orc_complex_conjugate_correction(orc *o);
 int orc_check_physfour_energy(orc *o, double atol, double *diff1, double *diff2);

@@ -154,7 +154,8 @@ struct spns_handle {
     double *phys = nullptr;
     void *edge = nullptr;                            // edge-correction planes (rotational form)
     void *inv_B1 = nullptr, *inv_B2 = nullptr;       // invariant spectra: advective-size work buffers (on first use)
-    double *inv_bins = nullptr;
+    double *inv_bins = nullptr;                      // 5 spectra, then the nu_t accumulators
+    double nut_stats[3] = {0.0, 0.0, 0.0};           // mean, rms, max of nu_t at the last invariant pass
     bool edge_axis[3] = {false, false, false};       // axes whose +-N/2 planes alias (M = 3h)
     std::map<int, void *> tw;                        // twiddle tables per length (precision of the handle)
     std::string err;

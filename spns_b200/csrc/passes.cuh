@@ -6,6 +6,9 @@
 #include "handle.h"
 
 #include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
 
 template <typename T> struct Passes {
     using C = spns::cx<T>;
@@ -172,14 +175,16 @@ template <typename T> struct Passes {
         if (!h->inv_B1) {
             CK(cudaMallocAsync(&h->inv_B1, sizeof(C) * 6 * (size_t)g.S1, h->st));
             CK(cudaMallocAsync(&h->inv_B2, sizeof(C) * 9 * (size_t)g.S2, h->st));
-            CK(cudaMallocAsync((void **)&h->inv_bins, sizeof(double) * 5 * nb, h->st));
+            CK(cudaMallocAsync((void **)&h->inv_bins, sizeof(double) * (5 * nb + 3), h->st));
         }
+        double *nut = h->inv_bins + 5 * nb;               // nu_t sum, sum of squares, max bits
+        CK(cudaMemsetAsync(nut, 0, sizeof(double) * 3, h->st));
         std::swap(h->B1, h->inv_B1);
         std::swap(h->B2, h->inv_B2);
         auto passes = [&]() -> int {
             DISPATCH(g.Mx, LAUNCH((launch_k1<LL, spns::MODE_INV>(h))));
             DISPATCH(g.My, LAUNCH((launch_k2<LL, spns::MODE_INV>(h))));
-            DISPATCH(g.Mz, LAUNCH((launch_k3<LL, spns::MODE_INV>(h, nullptr))));
+            DISPATCH(g.Mz, LAUNCH((launch_k3<LL, spns::MODE_INV>(h, nut))));
             DISPATCH(g.My, LAUNCH((launch_k4<LL, spns::MODE_INV>(h))));
             DISPATCH(g.Mx, LAUNCH((launch_k5<LL, spns::MODE_INV>(h))));
             return SPNS_OK;
@@ -196,8 +201,18 @@ template <typename T> struct Passes {
                 g, (const C *)h->inv_B2 + (long long)c * g.S0, scale, h->last_rad_max, h->inv_bins + (long long)c * nb);
             CKL();
         }
-        CK(cudaMemcpyAsync(out, h->inv_bins, sizeof(double) * 5 * nb, cudaMemcpyDeviceToHost, h->st));
+        std::vector<double> host((size_t)5 * nb + 3);
+        CK(cudaMemcpyAsync(host.data(), h->inv_bins, sizeof(double) * host.size(), cudaMemcpyDeviceToHost, h->st));
         CK(cudaStreamSynchronize(h->st));
+        if (out) std::copy(host.begin(), host.begin() + 5 * nb, out);
+        const double npts = (double)g.Mx * g.My * g.Mz;
+        unsigned long long mb;
+        std::memcpy(&mb, &host[5 * nb + 2], sizeof(mb));
+        double mx;
+        std::memcpy(&mx, &mb, sizeof(mx));
+        h->nut_stats[0] = host[5 * nb] / npts;
+        h->nut_stats[1] = std::sqrt(host[5 * nb + 1] / npts);
+        h->nut_stats[2] = mx;
         return SPNS_OK;
     }
 

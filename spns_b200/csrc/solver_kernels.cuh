@@ -267,6 +267,23 @@ __device__ __forceinline__ void block_sum(double v, double *dst) {
     __syncthreads();
 }
 
+// Block maximum of a non-negative double, folded into *dst (its bits order as the values do).
+__device__ __forceinline__ void block_max_bits(double v, unsigned long long *dst) {
+    __shared__ double red[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        v = lane < nw ? red[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (lane == 0) atomicMax(dst, (unsigned long long)__double_as_longlong(v));
+    }
+    __syncthreads();
+}
+
 // Forward transform of the register pair z = a + i b and extraction of both
 // half spectra for kz < Kz:  Xa = (Z_k + conj Z_{L-k})/2, Xb = (Z_k - conj Z_{L-k})/(2i).
 // With jz: Xa += i kz Xb (the z-derivative of b folded into a; SGS divergence).
@@ -536,10 +553,13 @@ __global__ void __launch_bounds__(P *(L / E), K3MinBlocks<T, MODE, P *(L / E)>::
         }
     } else if constexpr (MODE == MODE_INV) {
         // Velocity-gradient invariants (src/HIT_LES.cpp:1297-1319, definitions
-        // src/tensor_algebra.cpp:165-306, 356-358) of G_ij = d_j u_i.
+        // src/tensor_algebra.cpp:165-306, 356-358) of G_ij = d_j u_i, and the
+        // eddy-viscosity statistics of the grid: `phys` holds 3 accumulators here
+        // (sum of nu_t, sum of nu_t^2, bits of the maximum nu_t).
         // S2 inputs as in the advective form: 0 u, 1 v, 2 w, 3 du/dx, 4 dv/dx, 5 dw/dx,
         // 6 du/dy, 7 dv/dy, 8 dw/dy; z-derivatives formed here.  Slots s = 3 i + j hold G_ij.
         // Outputs (S2 fields 0..4): Q_G, Q_S, R_G, R_S, V^2 forward-transformed, kz <= hz.
+        double nut_sum = 0.0, nut_sq = 0.0, nut_max = 0.0;
         cx<T> A[E];
         T rg[NREG > 0 ? NREG : 1][E];
 #pragma unroll
@@ -616,11 +636,27 @@ __global__ void __launch_bounds__(P *(L / E), K3MinBlocks<T, MODE, P *(L / E)>::
                 return d;
             };
             const double QG = 0.5 * (trG * trG - trGG), QS = 0.5 * (trS * trS - trSS);
+            // eddy viscosity of this grid point (src/HIT_LES.cpp:130-142, same expression order)
+            {
+                double ne = 2.0 * G[0][0] * G[0][0];
+                ne += 2.0 * G[1][1] * G[1][1];
+                ne += 2.0 * G[2][2] * G[2][2];
+                ne += (G[0][1] + G[1][0]) * (G[0][1] + G[1][0]);
+                ne += (G[0][2] + G[2][0]) * (G[0][2] + G[2][0]);
+                ne += (G[1][2] + G[2][1]) * (G[1][2] + G[2][1]);
+                const double nt = ok ? c.les_ct * sqrt(ne) : 0.0;
+                nut_sum += nt; nut_sq += nt * nt; nut_max = fmax(nut_max, nt);
+            }
             PH(0, row) = T(QG);
             PH(1, row) = T(QS);
             PH(2, row) = T(det3(G));
             PH(3, row) = T(det3(S));
             PH(4, row) = T(4.0 * (trS2O2 - 2.0 * QS * (QG - QS)));
+        }
+        if (phys) {
+            block_sum(nut_sum, phys);
+            block_sum(nut_sq, phys + 1);
+            block_max_bits(nut_max, reinterpret_cast<unsigned long long *>(phys + 2));
         }
 #pragma unroll 1
         for (int j = 0; j < 3; j++) {

@@ -845,6 +845,14 @@ int spns_invariant_spectra(spns_handle *h, double *spectra) {
     return spns_ops(h).invariant_spectra(h, spectra);
 }
 
+int spns_eddy_viscosity_stats(spns_handle *h, double *stats) {
+    if (!h || !stats) return SPNS_ERR_INVALID_ARGUMENT;
+    const int r = spns_ops(h).invariant_spectra(h, nullptr);
+    if (r) return r;
+    for (int i = 0; i < 3; i++) stats[i] = h->nut_stats[i];
+    return SPNS_OK;
+}
+
 int spns_estimate_device_bytes(const spns_hit_args *args, size_t *bytes) {
     if (!args || !bytes) return spns_fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "null argument");
     Geo g;

@@ -33,7 +33,7 @@ EXPORTED_SYMBOLS = (
     "spns_energy_cascade_noalloc_f64", "spns_estimate_device_bytes", "spns_seed_field", "spns_step_async",
     "spns_query", "spns_synchronize", "spns_checkpoint_bytes", "spns_checkpoint_save", "spns_checkpoint_load",
     "spns_ensemble_create", "spns_ensemble_step", "spns_ensemble_destroy", "spns_ensemble_last_error",
-    "spns_invariant_spectra", "spns_autotune", "spns_autotune_forget", "spns_set_shapes",
+    "spns_invariant_spectra", "spns_eddy_viscosity_stats", "spns_autotune", "spns_autotune_forget", "spns_set_shapes",
 )
 
 
@@ -137,6 +137,7 @@ def lib():
         L.spns_ensemble_last_error.argtypes = [vp]
         L.spns_ensemble_last_error.restype = C.c_char_p
         L.spns_invariant_spectra.argtypes = [vp, dp]
+        L.spns_eddy_viscosity_stats.argtypes = [vp, dp]
         L.spns_autotune.argtypes = [vp, i, ip]
         L.spns_autotune_forget.argtypes = []
         L.spns_set_shapes.argtypes = [vp, ip]
@@ -351,6 +352,12 @@ class HIT:
         n = C.c_int()
         self._ck(self._L.spns_kernels_per_step(self._h, C.byref(n)))
         return n.value
+
+    def eddy_viscosity_stats(self) -> np.ndarray:
+        """Mean, rms and maximum over the grid of nu_t (src/HIT_LES.cpp:130-142) of the current state."""
+        out = np.zeros(3)
+        self._ck(self._L.spns_eddy_viscosity_stats(self._h, _dp(out)))
+        return out
 
     # --- launch-shape autotuner ---
     def autotune(self, steps: int = 3):

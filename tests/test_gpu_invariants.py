@@ -59,3 +59,20 @@ def test_fp32_invariants_and_the_run_is_untouched(tmp_path):
     a.New_Fractional_Step_Method(3)
     c.New_Fractional_Step_Method(3)
     assert np.array_equal(a.get_compact(), c.get_compact())
+
+
+@pytest.mark.parametrize("N", [32, 48])
+def test_eddy_viscosity_stats_match_the_oracle(N):
+    import oracle as O
+    from spns_b200.hit import HIT
+    args = make_args(N, nu=3.283e-4, les=0.17)
+    gpu = HIT(args, k41_ranks=4)
+    ref = O.OracleHIT(args, k41_ranks=4)
+    for _ in range(3):
+        gpu.New_Fractional_Step_Method()
+        ref.New_Fractional_Step_Method()
+    g, r = gpu.eddy_viscosity_stats(), ref.eddy_viscosity_stats()
+    assert np.all(r > 0)
+    assert np.max(np.abs(g - r) / r) < 1e-11, (g, r)
+    dns = HIT(make_args(N, nu=3.283e-4), k41_ranks=4)
+    assert np.all(dns.eddy_viscosity_stats() == 0.0)
