@@ -85,3 +85,40 @@ def test_reference_driver_qa(name, tmp_path):
         for i in (2, 3, 4):                                     # Dt, Ek, Om %e (7 digits)
             assert abs(g[i] - e[i]) <= 1.5e-6 * abs(e[i]) + 1e-300
         assert abs(g[5] - e[5]) <= 1.5e-3                       # ReLambda %8.3f
+
+
+@pytest.mark.gpu
+def test_reference_driver_writes_invariant_spectra(tmp_path):
+    """VelGradInv_Spectra 1 with an output frequency: the unchanged driver writes the
+    per-frequency and final QG/QS/RG/RS/V2 files (src/MAIN.cpp:460-469, 497-503);
+    the final ones equal the oracle's spectra after the same steps to the 6 digits
+    the reference's writer prints."""
+    import oracle as O
+    from qa_util import load_case
+    if not os.path.exists(EXE):
+        pytest.fail("drop-in driver not built (make -C spns_b200/dropin)")
+    name = "TEST_1_DHIT_DNS"
+    _stage(name, str(tmp_path))
+    p = tmp_path / "params"
+    txt = re.sub(r"^Final_Time\s+\S+", "Final_Time\t0.1", p.read_text(), flags=re.M)
+    p.write_text(txt + "\nVelGradInv_Spectra\t1\nVelGradInv_Spectra_Freq\t2\nSpectra_Folder\tOUTPUT\n")
+    r = subprocess.run([EXE, "params"], cwd=str(tmp_path), capture_output=True, timeout=120)
+    out = r.stdout.decode(errors="replace") + r.stderr.decode(errors="replace")
+    assert r.returncode == 0, out[-3000:]
+    with open(os.path.join(str(tmp_path), "stdout.0"), errors="replace") as fh:
+        _, final = _parse(fh.read())
+    nsteps = int(final["Final time-steps"])
+    names = ("QG", "QS", "RG", "RS", "V2")
+    for i in range(nsteps // 2):
+        for nm in names:
+            assert (tmp_path / "OUTPUT" / f"{nm}_{i:08d}.dat").exists()
+    args, uvw, _ = load_case(name)
+    ref = O.OracleHIT(args, file_uvw=uvw)
+    for _ in range(nsteps):
+        ref.New_Fractional_Step_Method()
+    sp = ref.Recalculate_Invariants_Distribution()
+    for c, nm in enumerate(names):
+        rows = np.loadtxt(tmp_path / "OUTPUT" / f"{nm}.dat")
+        assert rows.shape == (sp.shape[1], 2) and np.array_equal(rows[:, 0], np.arange(sp.shape[1]))
+        m = np.abs(sp[c]) > 1e-6 * np.abs(sp[c]).max()
+        assert np.max(np.abs(rows[m, 1] - sp[c][m]) / np.abs(sp[c][m])) < 2e-5, nm
