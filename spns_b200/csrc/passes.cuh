@@ -38,9 +38,12 @@ template <typename T> struct Passes {
     }
     template <int L, int MODE, int ALT = 0> static cudaError_t launch_k3(spns_handle *h, double *phys) {
         using S3 = Shape3<T, L, MODE, ALT>;
-        constexpr bool STAGE = MODE == spns::MODE_ROT && ShapeSel<T>::Z_STAGE;
+        constexpr bool STAGE_ROT = MODE == spns::MODE_ROT && ShapeSel<T>::Z_STAGE;
+        constexpr bool STAGE_LES = MODE == spns::MODE_LES && sizeof(T) == 4 && SPNS_F32_Z_STAGE_LES;
+        constexpr bool STAGE = STAGE_ROT || STAGE_LES;
         auto kern = spns::k3_z<T, L, S3::E, S3::P, MODE, STAGE>;
-        const size_t smem = S3::SMEM + (STAGE ? (size_t)S3::P * 2 * spns::K3StagePairs<T>::N * h->g.Kz * sizeof(C) : 0);
+        const size_t stage_fields = STAGE_ROT ? 2 * spns::K3StagePairs<T>::N : STAGE_LES ? 9 : 0;
+        const size_t smem = S3::SMEM + (size_t)S3::P * stage_fields * h->g.Kz * sizeof(C);
         cudaError_t e = spns_set_smem(kern, smem);
         if (e != cudaSuccess) return e;
         const long long npen = (long long)h->g.Mx * h->g.My;

@@ -397,6 +397,12 @@ template <int MODE> struct K3Phys { static constexpr int N = MODE == MODE_ADV ? 
 #define SPNS_F32_Z_STAGE_PAIRS 3
 #endif
 template <typename T> struct K3StagePairs { static constexpr int N = sizeof(T) == 8 ? SPNS_Z_STAGE_PAIRS : SPNS_F32_Z_STAGE_PAIRS; };
+#ifndef SPNS_F32_Z_STAGE_LES
+#define SPNS_F32_Z_STAGE_LES 1    // single-precision LES z pass: stage the nine input fields in shared memory
+#endif
+// Staging slot of S2 input field f (0 u, 1 v, 2 w, 3-5 d/dx, 6-8 d/dy) in the LES z pass:
+// the order of first use by the pairs, 0 1 2 3 6 4 7 5 8.
+__host__ __device__ constexpr int k3_stage_slot(int f) { return f <= 3 ? f : f == 6 ? 4 : f == 4 ? 5 : f == 7 ? 6 : f == 5 ? 7 : 8; }
 template <typename T, int MODE, int E = 12> struct K3Reg {
     // with few values per thread (E <= 6) more slots fit in registers
     static constexpr int R = E <= 6 ? (sizeof(T) == 8 ? 8 : 12) : sizeof(T) == 8 ? SPNS_K3_REG_SLOTS : SPNS_F32_K3_REG_SLOTS;
@@ -694,11 +700,43 @@ __global__ void __launch_bounds__(P *(L / E), K3MinBlocks<T, MODE, P *(L / E)>::
             for (int e = 0; e < E; e++) rg[i][e] = T(0);
 #define PH(slot, row) k3_slot<(slot), NREG, L, T, E>(rg, ph, e, row)
         // inverse pairs: (u, v), (w, du/dz), (du/dx, du/dy), (dv/dx, dv/dy), (dw/dx, dw/dy), (dv/dz, dw/dz)
+        // STAGE (single-precision LES): the nine input fields of the block's pencils are
+        // copied into shared memory asynchronously at the start, in five groups in the
+        // order the pairs first use them ({u, v}, {w}, {du/dx, du/dy}, {dv/dx, dv/dy},
+        // {dw/dx, dw/dy}), so later pairs' loads overlap the earlier transforms.
+        // Field f sits in staging slot K3StageSlot(f) of its pencil.
+        cx<T> *const st = reinterpret_cast<cx<T> *>(reinterpret_cast<T *>(smc + P * SmPencil<T, L, E>::PITCH) +
+                                                    (long long)P * K3Reg<T, MODE, E>::NSM * L) + (long long)p * 9 * g.Kz;
+        if constexpr (STAGE) {
+#pragma unroll
+            for (int grp = 0; grp < 5; grp++) {
+#pragma unroll
+                for (int h2 = 0; h2 < 2; h2++) {
+                    const int f = grp == 0 ? h2 : grp == 1 ? (h2 == 0 ? 2 : -1) : (h2 == 0 ? grp + 1 : grp + 4);
+                    if (f >= 0 && ok)
+                        for (int k = q; k < g.Kz; k += Q) cp_async_elem<T>(st + k3_stage_slot(f) * g.Kz + k, F(f) + k);
+                }
+                cp_async_commit();
+            }
+        }
 #pragma unroll 1
         for (int pi = 0; pi < 6; pi++) {
             const int fa = pi == 0 ? 0 : pi == 1 ? 2 : pi == 5 ? 1 : pi + 1;
             const int fb = pi == 0 ? 1 : pi == 1 ? 0 : pi == 5 ? 2 : pi + 4;
-            k3_load_pair<T, L, E>(A, F(fa), pi == 5, F(fb), pi == 1 || pi == 5, g.Kz, sz, q, ok);
+            if constexpr (STAGE) {
+                switch (pi) {
+                case 0: cp_async_wait<4>(); break;
+                case 1: cp_async_wait<3>(); break;
+                case 2: cp_async_wait<2>(); break;
+                case 3: cp_async_wait<1>(); break;
+                default: cp_async_wait<0>(); break;
+                }
+                __syncthreads();
+                k3_load_pair<T, L, E>(A, st + k3_stage_slot(fa) * g.Kz, pi == 5, st + k3_stage_slot(fb) * g.Kz, pi == 1 || pi == 5,
+                                      g.Kz, sz, q, ok);
+            } else {
+                k3_load_pair<T, L, E>(A, F(fa), pi == 5, F(fb), pi == 1 || pi == 5, g.Kz, sz, q, ok);
+            }
             fft<T, L, E, true, SmPencil<T, L, E>, (32 % (L / E) == 0)>(A, sm, q, tw);
             switch (pi) {
             case 0:
