@@ -209,6 +209,75 @@ def _timed_steps(h, n: int) -> float:
     return time.perf_counter() - t0
 
 
+def fp32_accuracy_block(a, local: int, rank: int, steps: int):
+    """FP32 compensated form against the FP64 form over `steps` steps of the benchmark box
+    from the same seeded state: E(K) per shell, total energy and dissipation nu*Omega
+    (Omega = sum of 2 k^2 E, the enstrophy integral of src/HIT_LES.cpp:490-495, 998-1002,
+    so that nu*Omega = 2 nu sum k^2 E(k)).  Each form runs alone."""
+    import numpy as np
+    from spns_b200.hit import HIT, SPNS_FP64, SPNS_FP32_HILO
+    from spns_b200.fields import seeded_spectral_field
+    res = {}
+    for prec in (SPNS_FP64, SPNS_FP32_HILO):
+        h = HIT(a, device=local, eps_forcing=EPS, precision=prec)
+        U0 = seeded_spectral_field(a.Nx, a.Ny, a.Nz, kp=KP, seed=SEED + rank)
+        h.set_compact(U0)
+        del U0
+        h.Recalculate_Velocity_Antitransform()
+        h.Recalculate_TimeStep()
+        h.New_Fractional_Step_Method(steps)
+        ek = h.Recalculate_Energy_Cascade()
+        om = h.Recalculate_Enstrophy()
+        res[prec] = (ek, float(np.sum(ek)), h.getnu() * om, h.gettime())
+        h.close()
+    e64, E64, d64, t64 = res[SPNS_FP64]
+    e32, E32, d32, t32 = res[SPNS_FP32_HILO]
+    m = e64 > 1e-6 * e64.max()
+    return {"steps": steps,
+            "ek_max_shell_rel_err": float(np.max(np.abs(e32[m] - e64[m]) / e64[m])),
+            "energy_rel_err": abs(E32 - E64) / E64,
+            "dissipation_rel_err": abs(d32 - d64) / d64,
+            "time_rel_err": abs(t32 - t64) / t64,
+            "fp64_energy": E64, "fp64_dissipation": d64,
+            "tolerance_ek_shell": 1e-5,
+            "shells_compared": "shells holding more than 1e-6 of the peak shell energy"}
+
+
+def same_n_block(local: int, n: int, threads: int, cpu_steps: int = 3, gpu_steps: int = 50):
+    """The oracle and the GPU on the SAME forced-DNS box at a size the host can hold
+    (N=n retained modes, FFT (3n/2)^3): measured steps/s of both, no extrapolation."""
+    from spns_b200.hit import HIT
+    from spns_b200.fields import seeded_spectral_field
+    import torch
+    s_cpu = cpu_sample(n, cpu_steps, threads)
+    a = box_args(n)
+    a.nu = nu_for(N_BOX)
+    h = HIT(a, device=local, eps_forcing=EPS)
+    h.set_compact(seeded_spectral_field(n, n, n, kp=KP, seed=SEED))
+    h.Recalculate_Velocity_Antitransform()
+    h.Recalculate_TimeStep()
+    h.New_Fractional_Step_Method(3)
+    stream = torch.cuda.ExternalStream(h.stream_handle(), device=torch.device("cuda", local))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    h._ck(h._L.spns_step(h._h, gpu_steps))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    gpu_s = e0.elapsed_time(e1) / 1e3 / gpu_steps
+    t0 = time.perf_counter()
+    for _ in range(gpu_steps):
+        h.New_Fractional_Step_Method()
+        h.Recalculate_Energy_Cascade()
+    e2e_s = (time.perf_counter() - t0) / gpu_steps
+    h.close()
+    return {"N": n, "fft_grid": (3 * n) // 2, "cores": threads, "kind": "port",
+            "cpu_steps": cpu_steps, "cpu_steps_per_s": 1.0 / s_cpu,
+            "gpu_steps": gpu_steps, "gpu_steps_per_s": 1.0 / gpu_s, "gpu_e2e_steps_per_s": 1.0 / e2e_s,
+            "gpu_over_cpu": s_cpu / gpu_s, "gpu_e2e_over_cpu": s_cpu / e2e_s,
+            "workload": f"the benchmark's forced DNS (same nu, eps, kappa scheme) at N={n}"}
+
+
 def ensemble_block(local: int, n_boxes: int = 64, steps: int = 500, seed: int = 7):
     """64 LES boxes of uneven size advanced together (one CUDA graph per step, FP32 form,
     launch shapes per box class picked by the autotuner).
@@ -465,6 +534,8 @@ def run_gpu(args):
                 "ek_max_abs_err_over_ek_tot": float(np.max(np.abs(ek32 - ek64)) / ek64.sum()),
                 "steps_compared": args.warmup + args.steps,
                 "shells_compared": "shells holding more than 1e-6 of the peak shell energy"}
+        if args.accuracy_steps > 0:
+            fp32["accuracy"] = fp32_accuracy_block(a, local, rank, args.accuracy_steps)
 
     if rank != 0:
         if dist is not None:
@@ -500,14 +571,16 @@ def run_gpu(args):
         "clocks": clk.summary(),
         "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 8 * nbins + 8,
-                "loop": "HIT.New_Fractional_Step_Method() + Recalculate_Energy_Cascade() (E(K) to host) per step"},
+                "loop": "HIT.New_Fractional_Step_Method() + Recalculate_Energy_Cascade() (E(K) to host) per step",
+                "why_no_h2d": "a step takes no host input: the state stays resident on the device between steps, "
+                              "as HIT keeps its fields in its own arrays in the reference's loop "
+                              "(src/MAIN.cpp:413-485); the initial state is uploaded once before the loop"},
         "gpu_launches": nk * args.steps,
         "kernel_ms": share,
         "kernel_ms_note": "per-kernel CUDA-event times of K further uncaptured steps on the solver stream",
         "graphs": "timed steps replay one CUDA graph per step",
         "step_algorithmic_bytes": step_bytes,
         "step_achieved_GBps": step_bytes / (ms_max / args.steps / 1e3) / 1e9,
-        "fp32_hilo": fp32,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                      "algorithmic_bytes": bytes_per[dom]},
@@ -520,6 +593,10 @@ def run_gpu(args):
         line["serving"] = serving_block(local, n_requests=args.serving_requests)
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_block(os.cpu_count() or 1)
+        if args.same_n:
+            line["cpu_baseline"]["measured_same_n"] = same_n_block(local, args.same_n, os.cpu_count() or 1)
+    # last: the driver keeps the tail of a long line
+    line["fp32_hilo"] = fp32
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -546,6 +623,10 @@ def main():
     ap.add_argument("--no-serving", action="store_true", help="skip the served-workload field")
     ap.add_argument("--no-les", action="store_true", help="skip the LES-configuration field (FP32 vs FP64)")
     ap.add_argument("--serving-requests", type=int, default=40)
+    ap.add_argument("--accuracy-steps", type=int, default=100,
+                    help="steps of the FP32-vs-FP64 accuracy comparison (0 skips it)")
+    ap.add_argument("--same-n", type=int, default=128,
+                    help="box size at which the oracle and the GPU are both measured (0 skips it)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -224,23 +224,28 @@ const char *spns_last_error(spns_handle *h);
 const char *spns_status_string(int status);
 
 /* Energy spectrum without device allocation.  No counterpart in the reference.
- * For callers that cannot allocate device memory when they need E(K): work
- * recorded into a CUDA graph (an allocation may synchronise the device, which
- * a captured stream forbids), frameworks that own all device memory through
- * their own pool, and loops that must not stall other streams.  Computes
- * Ek[K], K=0..nbins-1 (host array; K=round(|k|), conjugate weight 2 for kz>0,
- * as spns_recalculate_energy_cascade) and *ek_tot from a compact spectral
- * velocity already on the device (uvw_dev: 3 components one after another, each
- * Ky*Kx*Kz double2 in the layout of spns_get_spectral; wavenumbers scaled by
- * the length factors), on `stream` (cudaStream_t, NULL = default stream); it
+ * For callers that cannot allocate device memory when they need E(K): host
+ * frameworks that own all device memory through their own caching pool (a
+ * foreign cudaMalloc fails once the pool holds the free memory, or fragments
+ * it), and loops that must not stall other streams (cudaMalloc and cudaFree can
+ * synchronise the device).  Computes Ek[K], K=0..nbins-1 (host array;
+ * K=round(|k|), conjugate weight 2 for kz>0, as spns_recalculate_energy_cascade)
+ * and *ek_tot from a compact spectral velocity already on the device (uvw_dev:
+ * 3 components one after another, each Ky*Kx*Kz double2 in the layout of
+ * spns_get_spectral; wavenumbers scaled by the length factors), on `stream`
+ * (cudaStream_t, NULL = default stream).  It copies E(K) to the host and
  * synchronises that stream before returning.
+ * The input must be FP64 state (double2).  The compensated FP32 form keeps a
+ * float2 hi/lo pair, which this call cannot read: for such handles use
+ * spns_recalculate_energy_cascade.
  * Working memory is a fixed array of SPNS_NOALLOC_MAX_BINS x 2 doubles compiled
  * into the library (held by every device that loads it until exit); nbins
  * above SPNS_NOALLOC_MAX_BINS is rejected with SPNS_ERR_UNSUPPORTED_SIZE.  The
- * first call on a device looks the array up (cudaGetSymbolAddress) and should
- * come before any stream capture.  All calls share the array: calls whose GPU
- * work overlaps race and must be serialised by the caller.  Error text:
- * spns_last_error(NULL). */
+ * first call on a device looks up the array's device address and the device's
+ * SM count (cudaGetSymbolAddress, cudaDeviceGetAttribute) and keeps them for
+ * the life of the process: do not call it after cudaDeviceReset on that
+ * device.  All calls share the array: calls whose GPU work overlaps race and
+ * must be serialised by the caller.  Error text: spns_last_error(NULL). */
 #define SPNS_NOALLOC_MAX_BINS 2048
 int spns_energy_cascade_noalloc_f64(const void *uvw_dev, int Kx, int Ky, int Kz, int Lx_factor, int Ly_factor,
                                     int Lz_factor, double *Ek, int nbins, double *ek_tot, void *stream);

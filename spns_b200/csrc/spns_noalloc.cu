@@ -2,22 +2,25 @@
 // allocation.
 //
 // Some callers cannot call cudaMalloc when they need the spectrum:
-//   * code that records its work into a CUDA graph: cudaMalloc/cudaFree may
-//     synchronise the device, which is not allowed while a stream is captured;
 //   * a host framework that owns all device memory through its own pool (a
-//     caching allocator): a foreign cudaMalloc can fail or fragment that pool;
+//     caching allocator that has reserved the free memory): a foreign
+//     cudaMalloc then fails for want of memory, or fragments the pool;
 //   * a latency-critical loop that must not stall the other streams of the
-//     device with the implicit synchronisation of an allocation or free.
+//     device: cudaMalloc and cudaFree can synchronise the whole device.
 // For them spns_energy_cascade_noalloc_f64 computes E(K) straight from device
 // pointers they already own, with its working bins in a fixed array compiled
-// into the library.
+// into the library.  The call copies E(K) to the host and synchronises the
+// given stream before it returns.
 //
 // The working array is a file-scope __device__ array of SPNS_NOALLOC_MAX_BINS
 // energy bins plus as many enstrophy bins (32 KiB): every GPU that loads the
 // library holds it until the process exits.  All calls on a device share it and
 // it keeps the contents of the last call, so each call clears it first; calls
 // whose work overlaps on the GPU (different streams, or different host threads
-// on one device) race on it and must be serialised by the caller.
+// on one device) race on it and must be serialised by the caller.  The array's
+// device address and the device's SM count are looked up once per device and
+// kept for the life of the process, so the entry point must not be used after
+// the host program calls cudaDeviceReset on that device.
 #include "spns.h"
 #include "solver_kernels.cuh"
 
@@ -37,16 +40,18 @@ namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 double *g_bins_addr[kMaxDevices] = {nullptr};
+int g_sm_count[kMaxDevices] = {0};
 
 int noalloc_fail(int code, const char *msg) {
     spns_set_handleless_error(msg);
     return code;
 }
 
-// Device address of the working array on the current device.  The host-side
-// symbol is only a stand-in for the array, so the address is looked up once per
-// device, with that device current, and cached.
-int bins_address(int dev, double **out) {
+// Device address of the working array on the current device, and the device's
+// SM count (grid size of the shell sums).  The host-side symbol is only a
+// stand-in for the array, so the address is looked up once per device, with
+// that device current, and cached.
+int bins_address(int dev, double **out, int *sms) {
     if (dev < 0 || dev >= kMaxDevices) return noalloc_fail(SPNS_ERR_INVALID_ARGUMENT, "device ordinal out of range");
     std::lock_guard<std::mutex> lock(g_setup_mutex);
     if (!g_bins_addr[dev]) {
@@ -57,9 +62,14 @@ int bins_address(int dev, double **out) {
             snprintf(buf, sizeof(buf), "cudaGetSymbolAddress of the working bins failed: %s", cudaGetErrorString(e));
             return noalloc_fail(SPNS_ERR_CUDA, buf);
         }
+        int n = 0;
+        e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess || n < 1) return noalloc_fail(SPNS_ERR_CUDA, "cudaDeviceGetAttribute(SM count) failed");
+        g_sm_count[dev] = n;
         g_bins_addr[dev] = static_cast<double *>(p);
     }
     *out = g_bins_addr[dev];
+    *sms = g_sm_count[dev];
     return SPNS_OK;
 }
 } // namespace
@@ -78,7 +88,8 @@ extern "C" int spns_energy_cascade_noalloc_f64(const void *uvw_dev, int Kx, int 
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return noalloc_fail(SPNS_ERR_CUDA, cudaGetErrorString(e));
     double *bins = nullptr;
-    int rc = bins_address(dev, &bins);
+    int sms = 0;
+    int rc = bins_address(dev, &bins, &sms);
     if (rc) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
 
@@ -93,7 +104,8 @@ extern "C" int spns_energy_cascade_noalloc_f64(const void *uvw_dev, int Kx, int 
     e = cudaMemsetAsync(bins, 0, sizeof(double) * 2 * (size_t)nbins, st);
     if (e != cudaSuccess) return noalloc_fail(SPNS_ERR_CUDA, cudaGetErrorString(e));
     const long long n = g.S0;
-    const int blocks = (int)((n + 255) / 256 < 148 * 8 ? (n + 255) / 256 : 148 * 8);
+    const long long cap = 8LL * sms;   // 8 resident blocks of 256 threads per SM
+    const int blocks = (int)((n + 255) / 256 < cap ? (n + 255) / 256 : cap);
     k_shell_sums<double><<<blocks, 256, sizeof(double) * 2 * nbins, st>>>(
         g, (const cx<double> *)u, (const cx<double> *)(u + g.S0), (const cx<double> *)(u + 2 * g.S0), nullptr, nullptr, nullptr, nbins - 1, bins,
         bins + nbins);

@@ -167,6 +167,12 @@ static void pull_scalars(const HIT *self, spns_scalars &s) {
     } while (0)
 
 void HIT::New_Fractional_Step_Method() {
+#if (QA)
+    // The reference's QA build checks, before every step, that the energy of the
+    // spectral state equals that of its physical field to 1e-13 and crashes if not
+    // (src/HIT_LES.cpp:10-12, 1216-1252).
+    Check_PhysFour_Energy(1e-13);
+#endif
     SPNS_FORWARD(spns_step(h, 1), "New_Fractional_Step_Method");
     SPNS_PULL();
 }
@@ -239,6 +245,9 @@ void HIT::Check_PhysFour_Energy(const REAL atol) {
     int ok = 0;
     double d1 = 0.0, d2 = 0.0;
     SPNS_FORWARD(spns_check_physfour_energy(h, atol, &ok, &d1, &d2), "Check_PhysFour_Energy");
+    spns_scalars s;
+    pull_scalars(this, s);
+    Ek_Tot = s.Ek_Tot;   // the reference's check runs Recalculate_Energy (src/HIT_LES.cpp:1242)
     if (!ok) crash("Ek differences exceed tolerance [EkReal vs EkFour %e, EkSpNS vs EkFour: %e]\n", d1, d2);
 }
 

@@ -59,4 +59,8 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    # the reference checkout: first argument, else $SPNS_REFERENCE
+    src = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SPNS_REFERENCE", "")
+    if not src:
+        sys.exit("usage: make_fixtures.py <reference checkout>  (or set SPNS_REFERENCE)")
+    main(src)

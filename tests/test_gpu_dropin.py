@@ -122,3 +122,87 @@ def test_reference_driver_writes_invariant_spectra(tmp_path):
         assert rows.shape == (sp.shape[1], 2) and np.array_equal(rows[:, 0], np.arange(sp.shape[1]))
         m = np.abs(sp[c]) > 1e-6 * np.abs(sp[c]).max()
         assert np.max(np.abs(rows[m, 1] - sp[c][m]) / np.abs(sp[c][m])) < 2e-5, nm
+
+
+def _set_param(txt, key, value):
+    """Sets `key value` in a parameters file text (uncommenting or appending the line)."""
+    pat = re.compile(rf"^#?\s*{key}\s+\S+.*$", re.M)
+    if pat.search(txt):
+        return pat.sub(f"{key}\t{value}", txt, count=1)
+    return txt + f"\n{key}\t{value}\n"
+
+
+@pytest.mark.gpu
+def test_reference_driver_writes_fields_and_spectra(tmp_path):
+    """Velocity_Physical / Velocity_Fourier / Energy_Cascade outputs of the unchanged driver
+    (src/MAIN.cpp:452-484, 492-515; writers src/HIT_LES_output.cpp:8-115 and the
+    "K<TAB>Ek" file of src/HIT_LES.cpp:1180-1187), against the oracle after the same
+    steps; then the written physical field is read back as an initial field
+    (Binary_Input_Filename, src/HIT_LES.cpp:618-686, 738-763) and reproduces the state."""
+    import oracle as O
+    from qa_util import load_case
+    from gpu_util import rel_l2
+    from spns_b200.params import read_params, derive_hit_args
+    if not os.path.exists(EXE):
+        pytest.fail("drop-in driver not built (make -C spns_b200/dropin)")
+    name = "TEST_1_DHIT_DNS"
+    _stage(name, str(tmp_path))
+    p = tmp_path / "params"
+    txt = p.read_text()
+    for k, v in (("Final_Time", "0.05"), ("Velocity_Physical", 1), ("Velocity_Fourier", 1), ("Energy_Cascade", 1),
+                 ("Velocity_Phys_Freq", 2), ("Velocity_Four_Freq", 2), ("Energy_Cascade_Freq", 2),
+                 ("Spectra_Folder", "OUTPUT")):
+        txt = _set_param(txt, k, v)
+    p.write_text(txt)
+    r = subprocess.run([EXE, "params"], cwd=str(tmp_path), capture_output=True, timeout=120)
+    out = r.stdout.decode(errors="replace") + r.stderr.decode(errors="replace")
+    assert r.returncode == 0, out[-3000:]
+    with open(os.path.join(str(tmp_path), "stdout.0"), errors="replace") as fh:
+        _, final = _parse(fh.read())
+    nsteps = int(final["Final time-steps"])
+    assert nsteps >= 3
+    od = tmp_path / "OUTPUT"
+    # per-frequency files after step n (the driver's counter, src/MAIN.cpp:436): physical when
+    # n % 2 == 0, Fourier and spectra when (n+1) % 2 == 0
+    assert len(list(od.glob("Velocity_0*.bin"))) == nsteps // 2
+    assert len(list(od.glob("Velocity_Fourier_0*.bin"))) == (nsteps + 1) // 2
+    assert len(list(od.glob("Energy_Cascade_0*.dat"))) == (nsteps + 1) // 2
+
+    args, uvw, _ = load_case(name)
+    ref = O.OracleHIT(args, file_uvw=uvw)
+    for _ in range(nsteps):
+        ref.New_Fractional_Step_Method()
+    Uo = ref.get_compact()
+    ref.Recalculate_Velocity_Antitransform()
+    Po = ref.get_physical()
+    Eo = ref.Recalculate_Energy_Cascade()
+
+    Uf = np.fromfile(od / "Velocity_Fourier.bin", dtype="<f8").view(np.complex128).reshape(Uo.shape)
+    assert rel_l2(Uf, Uo) < 1e-12
+    Pf = np.fromfile(od / "Velocity.bin", dtype="<f8").reshape(Po.shape)
+    assert rel_l2(Pf, Po) < 1e-12
+    rows = np.loadtxt(od / "Energy_Cascade.dat")
+    assert rows.shape == (Eo.size, 2) and np.array_equal(rows[:, 0], np.arange(Eo.size))
+    m = Eo > 1e-12 * Eo.max()
+    assert np.max(np.abs(rows[m, 1] - Eo[m]) / Eo[m]) < 1e-5        # 6 printed digits
+    assert np.all(np.abs(rows[~m, 1]) <= 1e-10 * Eo.max())
+
+    # the physical field read back as an initial field (M^3 file: every retained mode survives the truncation)
+    M = Po.shape[1]
+    (tmp_path / "DATA").mkdir(exist_ok=True)
+    Pf.astype("<f8").tofile(tmp_path / "DATA" / "restart.bin")
+    txt2 = re.sub(r"^ASCII_Input_Filename.*$", "#", txt, flags=re.M)
+    for k, v in (("Binary_Input_Filename", "DATA/restart.bin"), ("Nx_file", M), ("Ny_file", M), ("Nz_file", M)):
+        txt2 = _set_param(txt2, k, v)
+    p2 = tmp_path / "params_restart"
+    p2.write_text(txt2)
+    a2 = derive_hit_args(read_params(str(p2)), base_dir=str(tmp_path))
+    ref2 = O.OracleHIT(a2, file_uvw=Pf)
+    assert rel_l2(ref2.get_compact(), Uo) < 1e-13
+    from spns_b200.hit import HIT
+    gpu2 = HIT(a2, file_uvw=Pf)
+    assert rel_l2(gpu2.get_compact(), Uo) < 1e-13
+    gpu2.close()
+    r = subprocess.run([EXE, "params_restart"], cwd=str(tmp_path), capture_output=True, timeout=120)
+    out = r.stdout.decode(errors="replace") + r.stderr.decode(errors="replace")
+    assert r.returncode == 0, out[-3000:]

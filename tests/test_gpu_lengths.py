@@ -1,0 +1,104 @@
+"""GPU step against the oracle at the FFT lengths the benchmark configurations run.
+
+The forced 512^3 DNS transforms at length 768, the LES configuration and the
+served N=256 runs at 384, the served N=128 runs at 192.  Each pass kernel is a
+separate instantiation per length (values per thread, threads per pencil,
+exchange layouts, warp or block barriers), so parity at 48..96 says nothing
+about them.  Reduced anisotropic boxes put one axis at the benchmark length and
+keep the oracle fast: (512, 32, 32) runs the x passes (K1, K5) at 768,
+(32, 512, 32) the y passes (K2, K4), (32, 32, 512) the z pass (K3).
+
+Initial field: energy in every retained mode, the +-N/2 planes included
+(`broadband_field`), so every row of every transform carries data and the
+aliasing correction of the rotational form is exercised from the first step.
+
+Forms, as in src/HIT_LES.cpp:9-25, 74-125, 130-192:
+- "bench": rotational form with the exact edge correction, kappa scheme, constant-power
+  forcing eps=0.1 on K=1..2 (the forced-DNS benchmark path);
+- "advective": the reference's u.grad(u) arithmetic, AB2, CFL step;
+- "les-rotating": Smagorinsky LES (C_s=0.17) in a frame rotating with Omega=(0,0,1).
+
+Bar: relative L2 of the spectral state <= 1e-12 after 10 steps, dt equal to 1e-13
+at every step, as for the short lengths.  The compensated FP32 form is compared
+with the FP64 form at length 768 on every axis: E(K) within 1e-5 per shell.
+"""
+import numpy as np
+import pytest
+
+from gpu_util import broadband_field, make_args, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+STEPS = 10
+
+BOXES = {
+    "x768": (512, 32, 32), "y768": (32, 512, 32), "z768": (32, 32, 512),
+    "x384": (256, 32, 32), "y384": (32, 256, 32), "z384": (32, 32, 256),
+    "xyz192": (128, 128, 128),
+}
+FORMS = {
+    "bench": (0, dict(self_adaptive=True), dict(eps_forcing=0.1)),
+    "advective": (2, dict(), dict()),
+    "les-rotating": (0, dict(les=0.17, rotating=(0.0, 0.0, 1.0)), dict()),
+}
+
+
+def _pair(box, form_name, seed):
+    import oracle as O
+    from spns_b200.hit import HIT
+    form, aopt, hopt = FORMS[form_name]
+    args = make_args(0, nu=3.283e-4, Ns=box, **aopt)
+    gpu = HIT(args, k41_ranks=1, nonlinear_form=form, **hopt)
+    ref = O.OracleHIT(args, k41_ranks=1, **hopt)
+    U0 = broadband_field(*box, seed=seed)
+    for h in (gpu, ref):
+        h.set_compact(U0)
+        h.Recalculate_Velocity_Antitransform()
+        h.Recalculate_TimeStep()
+    assert abs(gpu.getAt() - ref.getAt()) <= 1e-13 * ref.getAt()
+    return gpu, ref
+
+
+@pytest.mark.parametrize("form_name", list(FORMS))
+@pytest.mark.parametrize("box_name", list(BOXES))
+def test_step_parity_at_benchmark_lengths(box_name, form_name):
+    box = BOXES[box_name]
+    gpu, ref = _pair(box, form_name, seed=sum(box) + len(form_name))
+    for i in range(STEPS):
+        gpu.New_Fractional_Step_Method()
+        ref.New_Fractional_Step_Method()
+        assert abs(gpu.getAt() - ref.getAt()) <= 1e-13 * ref.getAt(), f"dt differs at step {i + 1}"
+    err = rel_l2(gpu.get_compact(), ref.get_compact())
+    eg, eo = gpu.Recalculate_Energy_Cascade(), ref.Recalculate_Energy_Cascade()
+    m = eo > 1e-10 * eo.max()
+    print(f"{box_name} {form_name}: state rel L2 {err:.3e}, E(K) max shell rel {np.max(np.abs(eg[m] - eo[m]) / eo[m]):.3e}")
+    assert err < TOL
+    assert abs(gpu.gettime() - ref.gettime()) <= 1e-13 * ref.gettime()
+    gpu.close()
+
+
+@pytest.mark.parametrize("box_name", ["x768", "y768", "z768"])
+def test_fp32_form_at_length_768(box_name):
+    """Compensated FP32 form against FP64, same broadband field, 20 CFL steps of the bench form."""
+    from spns_b200.hit import HIT, SPNS_FP64, SPNS_FP32_HILO
+    box = BOXES[box_name]
+    args = make_args(0, nu=3.283e-4, Ns=box, self_adaptive=True)
+    U0 = broadband_field(*box, seed=7)
+    runs = {}
+    for prec in (SPNS_FP64, SPNS_FP32_HILO):
+        h = HIT(args, precision=prec, eps_forcing=0.1)
+        h.set_compact(U0)
+        h.Recalculate_Velocity_Antitransform()
+        h.Recalculate_TimeStep()
+        h.New_Fractional_Step_Method(20)
+        runs[prec] = h
+    e64 = runs[SPNS_FP64].Recalculate_Energy_Cascade()
+    e32 = runs[SPNS_FP32_HILO].Recalculate_Energy_Cascade()
+    m = e64 > 1e-6 * e64.max()
+    rel = np.abs(e32[m] - e64[m]) / e64[m]
+    print(f"{box_name} FP32 vs FP64: E(K) max shell rel {rel.max():.3e}")
+    assert rel.max() < 1e-5
+    assert abs(runs[SPNS_FP32_HILO].gettime() - runs[SPNS_FP64].gettime()) <= 1e-5 * runs[SPNS_FP64].gettime()
+    for h in runs.values():
+        h.close()

@@ -1,9 +1,10 @@
 """The allocation-free energy spectrum entry point against the handle-based one.
 
 spns_energy_cascade_noalloc_f64 serves callers that cannot allocate device
-memory at the time they need E(K) (graph capture, foreign memory pools,
-latency-critical loops): its working bins live in a fixed array compiled into
-libspns.  It must give the same spectrum as spns_recalculate_energy_cascade
+memory at the time they need E(K): host frameworks whose caching pool holds the
+device's free memory, and loops that must not stall other streams with the
+synchronisation an allocation can cause.  Its working bins live in a fixed
+array compiled into libspns.  It must give the same spectrum as spns_recalculate_energy_cascade
 (the handle's cudaMalloc'd bins) on the same state, call after call, since the
 shared array keeps the previous call's contents.  This file is collected last.
 """
