@@ -28,7 +28,8 @@ typedef enum spns_status {
     SPNS_ERR_CUDA = -3,             /* a CUDA runtime call failed               */
     SPNS_ERR_OUT_OF_MEMORY = -4,    /* device allocation refused                */
     SPNS_ERR_NONFINITE = -5,        /* NaN/Inf met in the CFL maximum           */
-    SPNS_ERR_DOMAIN = -6            /* time-step angle outside [0, pi/2] (crash "Topt fail!") */
+    SPNS_ERR_DOMAIN = -6,           /* time-step angle outside [0, pi/2] (crash "Topt fail!") */
+    SPNS_ERR_TIMEOUT = -7           /* a bounded device-side wait gave up (staged copy never arrived) */
 } spns_status;
 
 typedef enum spns_precision {

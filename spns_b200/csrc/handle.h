@@ -7,6 +7,7 @@
 
 #include <type_traits>
 #include "edge_kernels.cuh"
+#include "zpass_staged.cuh"
 
 #include <cuda_runtime.h>
 
@@ -121,6 +122,49 @@ template <int L, int MODE> constexpr bool shape_alt_ok() {
 template <typename T, int L, int ALT> using ShapeK1A = typename std::conditional<ALT != 0, ShapeT<T, L, SPNS_ALT_E, ShapeSel<T>::K1_T>, ShapeK1<T, L>>::type;
 template <typename T, int L, int ALT> using ShapeK2A = typename std::conditional<ALT != 0, ShapeT<T, L, SPNS_ALT_E, ShapeSel<T>::K2_T>, ShapeK2<T, L>>::type;
 template <typename T, int L, int ALT> using ShapeK5A = typename std::conditional<ALT != 0, ShapeT<T, L, SPNS_ALT_E, ShapeSel<T>::K5_T>, ShapeK5<T, L>>::type;
+
+// Rotational z pass with pair-by-pair bulk-copy staging, persistent
+// (k3_rot_staged, zpass_warp.cuh): used at lengths from SPNS_ZS_MIN_L up to 768.
+// Per precision: E values per thread, PB pencils per block, SLOTS physical slots
+// in shared memory (of four), MINB resident blocks per SM for the register budget.
+#ifndef SPNS_ZS_MIN_L
+#define SPNS_ZS_MIN_L 768         // double: measured 14.65 against 14.93 ms at 768, slower at 384
+#endif
+#ifndef SPNS_F32_ZS_MIN_L
+#define SPNS_F32_ZS_MIN_L 100000  // single: off (12.29 against 11.61 ms at 768)
+#endif
+#ifndef SPNS_ZS_E
+#define SPNS_ZS_E 12
+#endif
+#ifndef SPNS_ZS_PB
+#define SPNS_ZS_PB 2
+#endif
+#ifndef SPNS_ZS_SLOTS
+#define SPNS_ZS_SLOTS 0
+#endif
+#ifndef SPNS_ZS_MINB
+#define SPNS_ZS_MINB 2
+#endif
+#ifndef SPNS_F32_ZS_E
+#define SPNS_F32_ZS_E 12
+#endif
+#ifndef SPNS_F32_ZS_PB
+#define SPNS_F32_ZS_PB 2
+#endif
+#ifndef SPNS_F32_ZS_SLOTS
+#define SPNS_F32_ZS_SLOTS 0
+#endif
+#ifndef SPNS_F32_ZS_MINB
+#define SPNS_F32_ZS_MINB 4
+#endif
+template <typename T, int L> struct ZStagedShape {
+    static constexpr bool D = sizeof(T) == 8;
+    static constexpr int E = D ? SPNS_ZS_E : SPNS_F32_ZS_E;
+    static constexpr int PB = D ? SPNS_ZS_PB : SPNS_F32_ZS_PB;
+    static constexpr int SLOTS = D ? SPNS_ZS_SLOTS : SPNS_F32_ZS_SLOTS;
+    static constexpr int MINB = D ? SPNS_ZS_MINB : SPNS_F32_ZS_MINB;
+    static constexpr bool ON = L >= (D ? SPNS_ZS_MIN_L : SPNS_F32_ZS_MIN_L) && L <= 768 && L % E == 0 && spns::n_stages(L, E) > 0;
+};
 
 // z pass: pencils per block limited by the shared memory of the exchange
 // buffer plus the physical fields kept per pencil.

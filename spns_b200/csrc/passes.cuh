@@ -36,7 +36,29 @@ template <typename T> struct Passes {
         kern<<<grid, S::THREADS, S::SMEM_ROW, h->st>>>(h->g, (const C *)h->B1, (C *)h->B2, tw(h, L));
         return cudaGetLastError();
     }
+    // Rotational z pass staged pair by pair with bulk copies (zpass_staged.cuh),
+    // persistent: one wave of blocks over the SMs.
+    template <int L> static cudaError_t launch_k3_staged(spns_handle *h) {
+        using ZS = ZStagedShape<T, L>;
+        using LY = spns::ZStagedLayout<T, L, ZS::E, ZS::PB, ZS::SLOTS>;
+        auto kern = spns::k3_rot_staged<T, L, ZS::E, ZS::PB, ZS::SLOTS, ZS::MINB>;
+        const size_t smem = LY::smem_bytes(h->g.Kz);
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        constexpr int THREADS = ZS::PB * LY::Q;
+        int dev = 0, sms = 0, per_sm = 0;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+        if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, THREADS, smem)) != cudaSuccess) return e;
+        if (per_sm < 1) return cudaErrorInvalidConfiguration;
+        const long long groups = ((long long)h->g.Mx * h->g.My + ZS::PB - 1) / ZS::PB;
+        long long blocks = (long long)sms * per_sm;
+        if (blocks > groups) blocks = groups;
+        kern<<<(unsigned)blocks, THREADS, smem, h->st>>>(h->g, (C *)h->B2, h->c, h->ds, tw(h, L));
+        return cudaGetLastError();
+    }
     template <int L, int MODE, int ALT = 0> static cudaError_t launch_k3(spns_handle *h, double *phys) {
+        if constexpr (MODE == spns::MODE_ROT && ALT == 0 && ZStagedShape<T, L>::ON) return launch_k3_staged<L>(h);
         using S3 = Shape3<T, L, MODE, ALT>;
         constexpr bool STAGE_ROT = MODE == spns::MODE_ROT && ShapeSel<T>::Z_STAGE;
         constexpr bool STAGE_LES = MODE == spns::MODE_LES && sizeof(T) == 4 && SPNS_F32_Z_STAGE_LES;

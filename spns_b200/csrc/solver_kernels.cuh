@@ -52,6 +52,7 @@ struct DevScalars {
     unsigned long long max_bits[4];      // max|u|, max|v|, max|w|, max(|u|/Ax+|v|/Ay+|w|/Az)
     long long iter;
     int nonfinite, domain_err;
+    int wait_timeout;                    // a bounded wait of a staged pass gave up (SPNS_ERR_TIMEOUT)
 };
 
 struct StepConsts {
@@ -555,7 +556,9 @@ __global__ void __launch_bounds__(P *(L / E), K3MinBlocks<T, MODE, P *(L / E)>::
 #pragma unroll
                 for (int e = 0; e < E; e++) A[e] = mk<T>(rs[4][e], T(0));
             }
-            k3_store_job<T, L, E>(A, sm, q, g.Kz, j == 0 ? F(0) : F(2), j == 0 ? F(1) : nullptr, false, j == 1, sz, ok, tw);
+            // c_z goes over w_x (field 3, consumed by the first pair): the forward y pass
+            // reads the rotational nonlinear term from fields 0, 1 and 3 (k4_in_field)
+            k3_store_job<T, L, E>(A, sm, q, g.Kz, j == 0 ? F(0) : F(3), j == 0 ? F(1) : nullptr, false, j == 1, sz, ok, tw);
         }
     } else if constexpr (MODE == MODE_INV) {
         // Velocity-gradient invariants (src/HIT_LES.cpp:1297-1319, definitions
@@ -868,6 +871,10 @@ __global__ void __launch_bounds__(P *(L / E), K3MinBlocks<T, MODE, P *(L / E)>::
 #undef F
 }
 
+// S2 field holding component f of the nonlinear term after the z pass: the
+// rotational form writes c_z over w_x (field 3), the others in order.
+template <int MODE> __host__ __device__ constexpr int k4_in_field(int f) { return (MODE == MODE_ROT && f == 2) ? 3 : f; }
+
 // ===========================================================================
 // K4: forward transform along y with ky truncation.  Block = (kz chunk, x).
 // LES: G_i += i ky t_i2 (SGS divergence, y part).
@@ -904,7 +911,7 @@ __global__ void __launch_bounds__(P *(L / E), AxisMinBlocks<T, 4>::N) k4_fwd_y(G
 #pragma unroll 1
         for (int f = 0; f < Fields<MODE>::NOUT; f++) {
             cx<T> r[E];
-            load_fft(r, f);
+            load_fft(r, k4_in_field<MODE>(f));
             store(r, f, r, false);
         }
     } else {

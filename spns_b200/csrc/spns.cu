@@ -78,6 +78,7 @@ static int check_flags(spns_handle *h) {
     CK(cudaStreamSynchronize(h->st));
     if (s.nonfinite) return spns_fail(h, SPNS_ERR_NONFINITE, "non-finite velocity met in the CFL maximum (iter %lld)", s.iter);
     if (s.domain_err) return spns_fail(h, SPNS_ERR_DOMAIN, "Topt fail! (time-step angle outside [0, pi/2])");
+    if (s.wait_timeout) return spns_fail(h, SPNS_ERR_TIMEOUT, "a staged z pass gave up waiting for its bulk copies (iter %lld)", s.iter);
     return SPNS_OK;
 }
 
@@ -350,6 +351,7 @@ const char *spns_status_string(int s) {
     case SPNS_ERR_OUT_OF_MEMORY: return "out of device memory";
     case SPNS_ERR_NONFINITE: return "non-finite value";
     case SPNS_ERR_DOMAIN: return "time-step angle out of range";
+    case SPNS_ERR_TIMEOUT: return "device-side wait timed out";
     default: return "unknown status";
     }
 }
