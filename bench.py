@@ -60,15 +60,15 @@ def algorithmic_bytes(N: int, self_adaptive: bool = True, word: int = 16, form: 
 
     S0 = compact spectral field, S1 = after the x transform, S2 = after the y
     transform (complex elements of `word` bytes).  Rotational form (default, exact
-    with the edge correction): K1 3 S0 -> 5 S1, K2 5 S1 -> 6 S2, K3 6 S2 -> 3 S2;
-    advective form: 3 S0 -> 6 S1, 6 S1 -> 9 S2, 9 S2 -> 3 S2.  Then K4 3 S2 -> 3 S1,
+    with the edge correction): K1 3 S0 -> 6 S1 (u and the vorticity), K2 6 S1 -> 6 S2,
+    K3 6 S2 -> 3 S2; advective form: 3 S0 -> 6 S1, 6 S1 -> 9 S2, 9 S2 -> 3 S2.  Then K4 3 S2 -> 3 S1,
     K5 3 S1 -> 3 S0 (nonlinear term G), K6 reads G, u, R^{n-1} (+ u^{n-1}) and writes
     R^n, u^{n+1}.  The edge correction moves O(M^2) bytes (negligible)."""
     Nx, Ny, Nz = shape or (N, N, N)
     Kx, Ky, Kz = 2 * (Nx // 2) + 1, 2 * (Ny // 2) + 1, Nz // 2 + 1
     Mx, My = (3 * Nx) // 2, (3 * Ny) // 2
     S0, S1, S2 = Ky * Kx * Kz, Ky * Mx * Kz, My * Mx * Kz
-    n1, n2 = (6, 9) if form == "advective" else (5, 6)
+    n1, n2 = (6, 9) if form == "advective" else (6, 6)
     return {
         "k1_inv_x": (3 * S0 + n1 * S1) * word,
         "k2_inv_y": (n1 * S1 + n2 * S2) * word,

@@ -8,12 +8,14 @@
 #include <type_traits>
 #include "edge_kernels.cuh"
 #include "zpass_staged.cuh"
+#include "axis_tma.cuh"
 
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <map>
 #include <string>
+#include <utility>
 #include <vector>
 
 // ---------------------------------------------------------------------------
@@ -166,6 +168,30 @@ template <typename T, int L> struct ZStagedShape {
     static constexpr bool ON = L >= (D ? SPNS_ZS_MIN_L : SPNS_F32_ZS_MIN_L) && L <= 768 && L % E == 0 && spns::n_stages(L, E) > 0;
 };
 
+// x/y passes with TMA-moved tiles (k_axis_tma, axis_tma.cuh): double precision,
+// lengths from SPNS_AX_TMA_MIN_L, E values per thread and P pencils per block.
+// Off by default: two whole-field tiles per block leave one block (8 warps) per
+// SM, and at N=512 the y pass took 11.65 ms against 7.03 ms for k2_inv_y (E=12,
+// 512 threads: 11.13 ms; P=4: 19.0 ms).  Build with -DSPNS_AX_TMA_MIN_L=384 to use it.
+#ifndef SPNS_AX_TMA_MIN_L
+#define SPNS_AX_TMA_MIN_L 100000
+#endif
+#ifndef SPNS_AX_TMA_E
+#define SPNS_AX_TMA_E 24
+#endif
+#ifndef SPNS_AX_TMA_P
+#define SPNS_AX_TMA_P 8
+#endif
+#ifndef SPNS_AX_TMA_R
+#define SPNS_AX_TMA_R 128        // rows per TMA box
+#endif
+template <typename T, int L> struct AxisTmaShape {
+    static constexpr int E = SPNS_AX_TMA_E, P = SPNS_AX_TMA_P;
+    static constexpr bool ON = sizeof(T) == 8 && L >= SPNS_AX_TMA_MIN_L && L % E == 0 && L % SPNS_AX_TMA_R == 0 &&
+                               spns::n_stages(L, E) > 0 && 2 * (size_t)L * P * sizeof(spns::cx<T>) + 160 <= 227 * 1024;
+    static constexpr size_t SMEM = 2 * (size_t)L * P * sizeof(spns::cx<T>) + 128 + 2 * sizeof(unsigned long long);
+};
+
 // z pass: pencils per block limited by the shared memory of the exchange
 // buffer plus the physical fields kept per pencil.
 template <typename T, int L, int MODE, int ALT = 0> struct Shape3 {
@@ -211,6 +237,8 @@ struct spns_handle {
     double nut_stats[3] = {0.0, 0.0, 0.0};           // mean, rms, max of nu_t at the last invariant pass
     bool edge_axis[3] = {false, false, false};       // axes whose +-N/2 planes alias (M = 3h)
     std::map<int, void *> tw;                        // twiddle tables per length (precision of the handle)
+    std::map<std::pair<int, const void *>, CUtensorMap> tmaps;   // TMA tensor maps per (pass, input buffer)
+    int sms = 0;                                     // SM count of the handle's device
     std::string err;
     int kernels_per_step = 0;
     int edge_launches = 0;                           // launches of the edge correction in the last step

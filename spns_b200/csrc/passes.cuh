@@ -5,6 +5,8 @@
 #pragma once
 #include "handle.h"
 
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -27,7 +29,105 @@ template <typename T> struct Passes {
         kern<<<grid, S::THREADS, S::SMEM_ROW, h->st>>>(h->g, U(h, 0), U(h, 1), U(h, 2), (C *)h->B1, tw(h, L));
         return cudaGetLastError();
     }
+    // ---- x/y passes with TMA-moved tiles (double precision, axis_tma.cuh) ----
+    // Tensor map {2*Kz doubles, rows, lines, fields} over an input buffer, cached per
+    // (pass, buffer) in the handle.  Box {2P, R, 1, 1}.
+    static cudaError_t axis_map(spns_handle *h, int pass, const void *in, int rows, int lines, int fields, long long row_stride,
+                                long long line_stride, long long field_stride, int P, int R, const CUtensorMap **out) {
+        const auto key = std::make_pair(pass, in);
+        auto it = h->tmaps.find(key);
+        if (it == h->tmaps.end()) {
+            static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+            if (!encode) {
+                void *fn = nullptr;
+                cudaDriverEntryPointQueryResult q;
+                cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+                if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn) return e != cudaSuccess ? e : cudaErrorNotSupported;
+                encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+            }
+            const size_t cs = sizeof(C);
+            cuuint64_t dims[4] = {(cuuint64_t)(2 * h->g.Kz), (cuuint64_t)rows, (cuuint64_t)lines, (cuuint64_t)fields};
+            cuuint64_t strides[3] = {(cuuint64_t)(row_stride * cs), (cuuint64_t)(line_stride * cs), (cuuint64_t)(field_stride * cs)};
+            cuuint32_t box[4] = {(cuuint32_t)(2 * P), (cuuint32_t)R, 1u, 1u};
+            cuuint32_t estr[4] = {1u, 1u, 1u, 1u};
+            CUtensorMap m;
+            CUresult r = encode(&m, sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
+                                const_cast<void *>(in), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+            it = h->tmaps.emplace(key, m).first;
+        }
+        *out = &it->second;
+        return cudaSuccess;
+    }
+    // Persistent launch of k_axis_tma: one wave of blocks (one per SM at this shared memory).
+    template <int L, bool INV>
+    static cudaError_t launch_axis_tma(spns_handle *h, const CUtensorMap *map, const spns::AxisArgs &a, C *out) {
+        using S = AxisTmaShape<T, L>;
+        auto kern = spns::k_axis_tma<T, L, S::E, S::P, INV>;
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM);
+        if (e != cudaSuccess) return e;
+        constexpr int THREADS = S::P * (L / S::E);
+        int per_sm = 0;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, THREADS, S::SMEM)) != cudaSuccess) return e;
+        if (per_sm < 1) return cudaErrorInvalidConfiguration;
+        const long long items = (long long)((a.Kz + S::P - 1) / S::P) * a.lines;
+        const long long blocks = std::min<long long>(items, (long long)h->sms * per_sm);
+        kern<<<(unsigned)blocks, THREADS, S::SMEM, h->st>>>(*map, a, out, tw(h, L), h->ds);
+        return cudaGetLastError();
+    }
+    // Shared-memory placement of an inverse tile needs the boxes from both ends not to overlap.
+    template <int L> static bool axis_tma_fits(int hh) {
+        const int R = SPNS_AX_TMA_R;
+        const int npos = (hh + R) / R, nneg = (hh + R - 1) / R;
+        return hh >= 1 && 2 * hh + 1 <= L && L - nneg * R >= npos * R;
+    }
+    template <int L, int MODE> static cudaError_t launch_k2_tma(spns_handle *h) {
+        using S = AxisTmaShape<T, L>;
+        const spns::Geo &g = h->g;
+        const int nin = (h->B1 == h->inv_B1 || MODE == spns::MODE_INV) ? 6 : h->nB1;
+        const CUtensorMap *map = nullptr;
+        cudaError_t e = axis_map(h, 2, h->B1, g.Ky, g.Mx, nin, (long long)g.Mx * g.Kz, g.Kz, g.S1, S::P, SPNS_AX_TMA_R, &map);
+        if (e != cudaSuccess) return e;
+        spns::AxisArgs a{};
+        a.h = g.hy; a.Kc = g.Ky; a.lines = g.Mx; a.Kz = g.Kz; a.nout = spns::Fields<MODE>::K2;
+        for (int f = 0; f < a.nout; f++) a.src |= (unsigned long long)(f < 6 ? f : f - 6) << (4 * f);
+        a.deriv_from = (MODE == spns::MODE_VEL || MODE == spns::MODE_ROT) ? 99 : 6;
+        a.s = g.sy; a.o_row = (long long)g.Mx * g.Kz; a.o_line = g.Kz; a.o_field = g.S2; a.rbox = SPNS_AX_TMA_R;
+        return launch_axis_tma<L, true>(h, map, a, (C *)h->B2);
+    }
+    template <int L, int MODE> static cudaError_t launch_k4_tma(spns_handle *h) {
+        using S = AxisTmaShape<T, L>;
+        const spns::Geo &g = h->g;
+        const int nin = MODE == spns::MODE_INV ? 9 : h->nB2;
+        const CUtensorMap *map = nullptr;
+        cudaError_t e = axis_map(h, 4, h->B2, g.My, g.Mx, nin, (long long)g.Mx * g.Kz, g.Kz, g.S2, S::P, SPNS_AX_TMA_R, &map);
+        if (e != cudaSuccess) return e;
+        spns::AxisArgs a{};
+        a.h = g.hy; a.Kc = g.Ky; a.lines = g.Mx; a.Kz = g.Kz; a.nout = spns::Fields<MODE>::NOUT;
+        for (int f = 0; f < a.nout; f++) a.src |= (unsigned long long)spns::k4_in_field<MODE>(f) << (4 * f);
+        a.deriv_from = 99;
+        a.s = g.sy; a.o_row = (long long)g.Mx * g.Kz; a.o_line = g.Kz; a.o_field = g.S1; a.rbox = SPNS_AX_TMA_R;
+        return launch_axis_tma<L, false>(h, map, a, (C *)h->B1);
+    }
+    template <int L, int MODE> static cudaError_t launch_k5_tma(spns_handle *h) {
+        using S = AxisTmaShape<T, L>;
+        const spns::Geo &g = h->g;
+        const int nin = MODE == spns::MODE_INV ? 6 : h->nB1;
+        const CUtensorMap *map = nullptr;
+        cudaError_t e = axis_map(h, 5, h->B1, g.Mx, g.Ky, nin, g.Kz, (long long)g.Mx * g.Kz, g.S1, S::P, SPNS_AX_TMA_R, &map);
+        if (e != cudaSuccess) return e;
+        spns::AxisArgs a{};
+        a.h = g.hx; a.Kc = g.Kx; a.lines = g.Ky; a.Kz = g.Kz; a.nout = spns::Fields<MODE>::NOUT;
+        for (int f = 0; f < a.nout; f++) a.src |= (unsigned long long)f << (4 * f);
+        a.deriv_from = 99;
+        a.s = g.sx; a.o_row = g.Kz; a.o_line = (long long)g.Kx * g.Kz; a.o_field = g.S0; a.rbox = SPNS_AX_TMA_R;
+        return launch_axis_tma<L, false>(h, map, a, (C *)h->B2);
+    }
+
     template <int L, int MODE, int ALT = 0> static cudaError_t launch_k2(spns_handle *h) {
+        if constexpr (AxisTmaShape<T, L>::ON && ALT == 0)
+            if (axis_tma_fits<L>(h->g.hy)) return launch_k2_tma<L, MODE>(h);
         using S = ShapeK2A<T, L, ALT>;
         auto kern = spns::k2_inv_y<T, L, S::E, S::P, MODE>;
         cudaError_t e = spns_set_smem(kern, S::SMEM_ROW);
@@ -74,6 +174,8 @@ template <typename T> struct Passes {
         return cudaGetLastError();
     }
     template <int L, int MODE, int ALT = 0> static cudaError_t launch_k4(spns_handle *h) {
+        if constexpr (AxisTmaShape<T, L>::ON && ALT == 0 && MODE != spns::MODE_LES)
+            if (2 * h->g.hy + 1 <= L) return launch_k4_tma<L, MODE>(h);
         using S = ShapeK2A<T, L, ALT>;
         auto kern = spns::k4_fwd_y<T, L, S::E, S::P, MODE>;
         cudaError_t e = spns_set_smem(kern, S::SMEM_ROW);
@@ -83,6 +185,8 @@ template <typename T> struct Passes {
         return cudaGetLastError();
     }
     template <int L, int MODE, int ALT = 0> static cudaError_t launch_k5(spns_handle *h) {
+        if constexpr (AxisTmaShape<T, L>::ON && ALT == 0 && MODE != spns::MODE_LES)
+            if (2 * h->g.hx + 1 <= L) return launch_k5_tma<L, MODE>(h);
         using S = ShapeK5A<T, L, ALT>;
         auto kern = spns::k5_fwd_x<T, L, S::E, S::P, MODE>;
         cudaError_t e = spns_set_smem(kern, S::SMEM_ROW);
@@ -158,7 +262,7 @@ template <typename T> struct Passes {
         const int nb = h->last_rad_max + 1;
         CK(cudaMemsetAsync(h->bins, 0, sizeof(double) * 2 * nb, h->st));
         const long long n = h->g.S0;
-        const int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 8);
+        const int blocks = (int)std::min<long long>((n + 255) / 256, 8LL * h->sms);
         spns::k_shell_sums<T><<<blocks, 256, sizeof(double) * 2 * nb, h->st>>>(h->g, U(h, 0), U(h, 1), U(h, 2), Ulo(h, 0), Ulo(h, 1),
                                                                               Ulo(h, 2), h->last_rad_max, h->bins, h->bins + nb);
         CKL();
@@ -167,7 +271,7 @@ template <typename T> struct Passes {
 
     static int forcing_scale(spns_handle *h, int last_eff, int nullify) {
         const long long n = h->g.S0;
-        const int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 16);
+        const int blocks = (int)std::min<long long>((n + 255) / 256, 16LL * h->sms);
         spns::k_forcing_scale<T><<<blocks, 256, 0, h->st>>>(h->g, U(h, 0), U(h, 1), U(h, 2), Ulo(h, 0), Ulo(h, 1), Ulo(h, 2), h->FT,
                                                            last_eff, nullify);
         CKL();
@@ -182,7 +286,7 @@ template <typename T> struct Passes {
 
     static int seed_draw(spns_handle *h, unsigned long long seed, int lim_x, int lim_y, int lim_z) {
         const long long n = h->g.S0;
-        const int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 16);
+        const int blocks = (int)std::min<long long>((n + 255) / 256, 16LL * h->sms);
         spns::k_seed_draw<T><<<blocks, 256, 0, h->st>>>(h->g, seed, lim_x, lim_y, lim_z, U(h, 0), U(h, 1), U(h, 2), Ulo(h, 0),
                                                        Ulo(h, 1), Ulo(h, 2));
         CKL();
@@ -220,7 +324,7 @@ template <typename T> struct Passes {
         if (r) return r;
         CK(cudaMemsetAsync(h->inv_bins, 0, sizeof(double) * 5 * nb, h->st));
         const double scale = h->c.inv_norm * h->c.inv_norm;
-        const int blocks = (int)std::min<long long>((g.S0 + 255) / 256, 148 * 8);
+        const int blocks = (int)std::min<long long>((g.S0 + 255) / 256, 8LL * h->sms);
         for (int c = 0; c < 5; c++) {
             spns::k_shell_sums_scalar<T><<<blocks, 256, sizeof(double) * nb, h->st>>>(
                 g, (const C *)h->inv_B2 + (long long)c * g.S0, scale, h->last_rad_max, h->inv_bins + (long long)c * nb);
@@ -266,7 +370,7 @@ template <typename T> struct Passes {
             const long long n = (long long)es.R * es.C;
             C *V = (C *)h->edge, *Phi = V + 3 * (long long)np * n;
             const long long nb = n * 3 * np;
-            const int blocks = (int)std::min<long long>((nb + 255) / 256, 148 * 16);
+            const int blocks = (int)std::min<long long>((nb + 255) / 256, 16LL * h->sms);
             spns::k_edge_build<T><<<blocks, 256, 0, h->st>>>(g, U(h), es, V);
             CKL();
             DISPATCH(es.C, LAUNCH((launch_lines<LL, true>(h, V, (long long)es.R * 3 * np))));
@@ -275,7 +379,7 @@ template <typename T> struct Passes {
             CKL();
             DISPATCH(es.C, LAUNCH((launch_lines<LL, false>(h, Phi, (long long)es.R * np))));
             DISPATCH(es.R, LAUNCH((launch_cols<LL, false>(h, Phi, es.C, np))));
-            const int ablocks = (int)std::min<long long>((n * 2 + 255) / 256, 148 * 8);
+            const int ablocks = (int)std::min<long long>((n * 2 + 255) / 256, 8LL * h->sms);
             spns::k_edge_apply<T><<<dim3(ablocks, es.naxes), 256, 0, h->st>>>(g, (C *)h->B2, es, Phi);
             CKL();
             h->edge_launches += 7;

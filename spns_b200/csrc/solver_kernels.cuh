@@ -86,7 +86,7 @@ template <typename T, int PASS> struct AxisMinBlocks {
 
 // Field counts of the work buffers per mode.
 template <int MODE> struct Fields {
-    static constexpr int K1 = MODE == MODE_VEL ? 3 : MODE == MODE_ROT ? 5 : 6;  // S1 after the inverse x pass
+    static constexpr int K1 = MODE == MODE_VEL ? 3 : 6;                          // S1 after the inverse x pass
     static constexpr int K2 = MODE == MODE_VEL ? 3 : MODE == MODE_ROT ? 6 : 9;  // S2 after the inverse y pass
     static constexpr int K4 = MODE == MODE_LES ? 6 : MODE == MODE_INV ? 5 : 3;  // S1 after the forward y pass
     static constexpr int NOUT = MODE == MODE_INV ? 5 : 3;                       // compact outputs of the forward x pass
@@ -94,7 +94,8 @@ template <int MODE> struct Fields {
 
 // ===========================================================================
 // K1: inverse transform along x.  Block = (kz chunk, iy).
-//   VEL: u,v,w   ROT: u,v,w, w_y=i(kz u-kx w), i kx v   ADV/LES: u,v,w, du/dx, dv/dx, dw/dx
+//   VEL: u,v,w   ROT: u,v,w and the vorticity w_x=i(ky w-kz v), w_y=i(kz u-kx w),
+//   w_z=i(kx v-ky u) (ky is the block's, kx the row's)   ADV/LES: u,v,w, du/dx, dv/dx, dw/dx
 // ===========================================================================
 template <typename T, int L, int E, int P, int MODE>
 __global__ void __launch_bounds__(P *(L / E), AxisMinBlocks<T, 1>::N) k1_inv_x(Geo g, const cx<T> *__restrict__ u, const cx<T> *__restrict__ v,
@@ -105,6 +106,7 @@ __global__ void __launch_bounds__(P *(L / E), AxisMinBlocks<T, 1>::N) k1_inv_x(G
     const int iy = blockIdx.y, kz = blockIdx.x * P + p;
     const bool ok = kz < g.Kz;
     const T kzf = T(g.sz * kz);
+    const T kyf = T(g.sy * (iy <= g.hy ? iy : iy - g.Ky));
     SmRowMajor<T, P> sm{reinterpret_cast<cx<T> *>(smraw), p};
     const long long rb = (long long)iy * g.Kx;
 #pragma unroll 1
@@ -122,8 +124,9 @@ __global__ void __launch_bounds__(P *(L / E), AxisMinBlocks<T, 1>::N) k1_inv_x(G
                 else if (f == 1) val = v[idx];
                 else if (f == 2) val = w[idx];
                 else if (MODE == MODE_ROT) {
-                    if (f == 3) { cx<T> a = u[idx], c = w[idx]; val = mul_i(mk<T>(kzf * a.x - kx * c.x, kzf * a.y - kx * c.y)); }
-                    else { val = mul_i(kx * v[idx]); }
+                    if (f == 3) { cx<T> b = v[idx], c = w[idx]; val = mul_i(mk<T>(kyf * c.x - kzf * b.x, kyf * c.y - kzf * b.y)); }
+                    else if (f == 4) { cx<T> a = u[idx], c = w[idx]; val = mul_i(mk<T>(kzf * a.x - kx * c.x, kzf * a.y - kx * c.y)); }
+                    else { cx<T> a = u[idx], b = v[idx]; val = mul_i(mk<T>(kx * b.x - kyf * a.x, kx * b.y - kyf * a.y)); }
                 } else { // x-derivatives
                     const cx<T> *src = f == 3 ? u : f == 4 ? v : w;
                     val = mul_i(kx * src[idx]);
@@ -142,7 +145,7 @@ __global__ void __launch_bounds__(P *(L / E), AxisMinBlocks<T, 1>::N) k1_inv_x(G
 
 // ===========================================================================
 // K2: inverse transform along y.  Block = (kz chunk, x).
-//   ROT: u,v,w, w_x=i(ky w-kz v), w_y, w_z=i kx v - i ky u
+//   ROT: u,v,w, w_x, w_y, w_z (formed by K1)
 //   ADV/LES: u,v,w, du/dx,dv/dx,dw/dx, du/dy,dv/dy,dw/dy
 // ===========================================================================
 template <typename T, int L, int E, int P, int MODE>
@@ -166,13 +169,8 @@ __global__ void __launch_bounds__(P *(L / E), AxisMinBlocks<T, 2>::N) k2_inv_y(G
             if (ok && m2 <= g.hy && m2 >= -g.hy) {
                 const cx<T> *F = in + (long long)(m2 >= 0 ? m2 : m2 + g.Ky) * g.Mx * g.Kz + col;
                 const T ky = T(g.sy * m2);
-                if (MODE == MODE_VEL) {
+                if (MODE == MODE_VEL || MODE == MODE_ROT) {
                     val = F[(long long)f * g.S1];
-                } else if (MODE == MODE_ROT) {
-                    if (f < 3) val = F[(long long)f * g.S1];
-                    else if (f == 3) { cx<T> vv = F[g.S1], ww = F[2 * g.S1]; val = mul_i(mk<T>(ky * ww.x - kzf * vv.x, ky * ww.y - kzf * vv.y)); }
-                    else if (f == 4) val = F[3 * g.S1];
-                    else { cx<T> a = F[4 * g.S1], uu = F[0]; val = a - mul_i(ky * uu); }
                 } else {
                     if (f < 6) val = F[(long long)f * g.S1];
                     else val = mul_i(ky * F[(long long)(f - 6) * g.S1]);

@@ -155,7 +155,7 @@ static int file_init(spns_handle *h, const double *file_uvw, std::vector<double2
     for (int c = 0; c < 3; c++) {
         for (long long i = 0; i < nf; i++) host_in[i] = make_double2(file_uvw[c * nf + i], 0.0);
         CK(cudaMemcpy(d_in, host_in.data(), sizeof(double2) * nf, cudaMemcpyHostToDevice));
-        const int blocks = 148 * 16;
+        const int blocks = 16 * h->sms;
         // z: lines (x,y), element stride 1 -> A[x][y][k3]
         k_dft_axis<<<blocks, 256>>>(d_in, d_a, nz, hzf, d_k, (long long)nx * ny, 1, nz, hzf, 1, 1, twz);
         CKL();
@@ -300,7 +300,7 @@ static BufferPlan buffer_plan(const spns_hit_args &a, const Geo &g, int last_rad
     const size_t cs = a.precision == SPNS_FP64 ? sizeof(double2) : sizeof(float2);
     const bool hilo = a.precision == SPNS_FP32_HILO;
     const bool rot = !a.isLES && a.nonlinear_form != 2;
-    p.nB1 = rot ? 5 : 6;
+    p.nB1 = 6;
     p.nB2 = rot ? 6 : 9;
     // planes k_i = +-h alias onto each other when M_i = 3 h_i (even number of retained modes)
     p.edge_axis[0] = g.hx > 0 && g.Mx <= 3 * g.hx;
@@ -415,6 +415,10 @@ int spns_create(const spns_hit_args *args, const double *file_uvw, spns_handle *
         const int prio = std::max(greatest, std::min(least, a.stream_priority));
         if (cudaStreamCreateWithPriority(&h->st, cudaStreamNonBlocking, prio) != cudaSuccess)
             return cleanup(spns_fail(nullptr, SPNS_ERR_CUDA, "stream creation failed"));
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            h->sms < 1)
+            return cleanup(spns_fail(nullptr, SPNS_ERR_CUDA, "SM count query failed"));
     }
     const BufferPlan bp = buffer_plan(a, g, h->last_rad_max);
     h->nB1 = bp.nB1;

@@ -114,11 +114,11 @@ __global__ void __launch_bounds__(PB *(L / E), MINB) k3_rot_staged(Geo g, cx<T> 
     static_assert(SLOTS_SM >= 0 && SLOTS_SM <= 4, "zero to four slots in shared memory");
     constexpr bool WARP = (32 % Q == 0);                      // a pencil never leaves its warp
     constexpr bool BULK = sizeof(cx<T>) == 16;                // double: 16-byte elements, bulk copies
-    extern __shared__ __align__(128) unsigned char smraw[];
+    extern __shared__ __align__(128) unsigned char smraw_zs[];
     const int tid = threadIdx.x, sub = tid / Q, q0 = tid % Q;
     const int Kz = g.Kz;
     const int KS = LY::stage_stride(Kz);
-    cx<T> *const smc = reinterpret_cast<cx<T> *>(smraw);
+    cx<T> *const smc = reinterpret_cast<cx<T> *>(smraw_zs);
     SmPencil<T, L, E> sm{smc + sub * LY::PITCH};
     cx<T> *const stA = smc + PB * LY::PITCH;                  // staging: field a of the pair
     cx<T> *const stB = stA + KS;                              // field b
