@@ -129,6 +129,55 @@ int spns_invariant_spectra(spns_handle *h, double *spectra);
  * statistics; they carry the FP32-against-FP64 comparison of an LES run. */
 int spns_eddy_viscosity_stats(spns_handle *h, double *stats);
 
+/* ---- Slab decomposition of one box over several GPUs (one process per GPU) ----
+ * Replaces the reference's FFTW-MPI transposed slab layout
+ * (src/FFTW_package.cpp:47-56: fftw_mpi_local_size_3d_transposed and the
+ * TRANSPOSED_OUT/IN plans; src/FFTW_package.h:60-64: local_n0 x planes in
+ * physical space, local_n1 ky rows in spectral space) and its one all-to-all
+ * per 3-D transform.  Rank `rank` of `nranks` holds the compact ky rows
+ * [y0, y0+ny) of the state, the x pass's rows and the spectral sweep; between
+ * the inverse and the forward y pass it holds the x planes [x0, x0+nx) (y and z
+ * passes).  Both splits are FFTW-MPI's default block, ceil(n/nranks) per rank
+ * (spns_slab_block).  A step is the reference's two transposes around the y/z
+ * passes as two all-to-alls of the staging arrays, made by the caller (NCCL, or
+ * any transport) between the phases:
+ *   SPNS_SLAB_A, all-to-all, [sum ds.ef over ranks], SPNS_SLAB_B,
+ *   all-to-all, max of the 4 CFL words and of nonfinite over ranks, SPNS_SLAB_C.
+ * The first time step: SPNS_SLAB_VEL_A, all-to-all, SPNS_SLAB_VEL_B, max of the
+ * CFL words, SPNS_SLAB_DT (HIT::Recalculate_Velocity_Antitransform and
+ * Recalculate_TimeStep, src/HIT_LES.cpp:60-69, 365-403).
+ * The all-to-all moves block s of the sender's staging array (offsets from the
+ * block sizes in rank order) to the receiver's staging array, block r from rank
+ * r in rank order; spns_slab_exchange gives the counts.  Slab handles run the
+ * advective arithmetic (nonlinear_form 2) or LES, with AB2 or the kappa scheme,
+ * rotation and constant-power forcing; the state is set with spns_set_spectral
+ * on the rank's rows ([3][ny][Kx][Kz]); conjugate correction, Re_lambda forcing,
+ * K41 and file initial fields are not available (SPNS_ERR_INVALID_ARGUMENT).
+ * spns_step is refused on a slab handle. */
+enum spns_slab_phase_id {
+    SPNS_SLAB_VEL_A = 0, SPNS_SLAB_VEL_B = 1, SPNS_SLAB_DT = 2,
+    SPNS_SLAB_A = 3, SPNS_SLAB_B = 4, SPNS_SLAB_C = 5
+};
+/* [start, start+count) of block `rank` when n items are split over nranks
+ * (FFTW-MPI's default block size ceil(n/nranks)); host only, no device needed. */
+int spns_slab_block(int n, int nranks, int rank, int *start, int *count);
+int spns_slab_create(const spns_hit_args *args, int nranks, int rank, spns_handle **out);
+/* This rank's rows and planes. */
+int spns_slab_layout(spns_handle *h, int *y0, int *ny, int *x0, int *nx);
+int spns_slab_phase(spns_handle *h, int phase);
+/* Element counts (complex values of the handle's precision) this rank sends to
+ * and receives from every rank in the exchange after `phase` (SPNS_SLAB_VEL_A,
+ * SPNS_SLAB_A or SPNS_SLAB_B): send[s], recv[s] for s < nranks. */
+int spns_slab_exchange(spns_handle *h, int phase, long long *send, long long *recv);
+/* The same counts for any box and rank without a handle (host only): nf fields,
+ * back = 0 for the ky-rows -> x-planes exchange, 1 for the way back. */
+int spns_slab_counts(int Ky, int Mx, int Kz, int nranks, int rank, int nf, int back, long long *send, long long *recv);
+/* Device staging arrays (send, recv; `elems` complex values each) and the device
+ * address of the solver scalars with the byte offsets of the fields the caller
+ * reduces: off[0] the 4 CFL words (uint64 bit patterns of non-negative doubles:
+ * their maximum is the integer maximum), off[1] nonfinite (int), off[2] ef (double). */
+int spns_slab_buffers(spns_handle *h, void **send, void **recv, size_t *elems, void **scalars, size_t *off);
+
 /* getters / HIT::setnu (src/HIT_LES.h:187-201) */
 int spns_get_scalars(spns_handle *h, spns_scalars *out);
 int spns_set_nu(spns_handle *h, double nu);

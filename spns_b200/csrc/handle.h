@@ -239,6 +239,15 @@ struct spns_handle {
     std::map<int, void *> tw;                        // twiddle tables per length (precision of the handle)
     std::map<std::pair<int, const void *>, CUtensorMap> tmaps;   // TMA tensor maps per (pass, input buffer)
     int sms = 0;                                     // SM count of the handle's device
+    // slab decomposition (spns_slab_create): this rank holds the compact ky rows
+    // [g.y0, g.y0 + g.Ky) of the state and, in the y and z passes, the x planes
+    // [x0, x0 + gx.Mx); B1 holds the x pass's rows, B1x/B2x the x planes' S1/S2
+    // fields (B2 = B2x, also the nonlinear term), XS/XR the all-to-all staging
+    int slab_ranks = 0, slab_rank = 0, x0 = 0;
+    spns::Geo gx;
+    void *B1x = nullptr, *XS = nullptr, *XR = nullptr;
+    size_t xelems = 0;                               // complex elements of XS and of XR
+    spns::SlabRanges yr, xr;                         // every rank's ky rows and x planes
     std::string err;
     int kernels_per_step = 0;
     int edge_launches = 0;                           // launches of the edge correction in the last step
@@ -330,6 +339,7 @@ struct PrecOps {
     int (*conj_correction)(spns_handle *h);                   // kz=0 conjugate correction
     int (*seed_draw)(spns_handle *h, unsigned long long seed, int lim_x, int lim_y, int lim_z); // Philox field, unscaled
     int (*invariant_spectra)(spns_handle *h, double *out);    // 5 spectra of the gradient invariants
+    int (*slab_phase)(spns_handle *h, int phase);             // one phase of a slab-decomposed step
 };
 extern const PrecOps spns_ops_f64;
 extern const PrecOps spns_ops_f32;

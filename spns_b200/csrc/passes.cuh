@@ -446,7 +446,118 @@ template <typename T> struct Passes {
 #undef MARK
     }
 
+    // ---- slab decomposition (spns_slab_phase) ----
+    // Reorder between a [nf][n1][n2][Kz] array and the all-to-all staging blocks.
+    static cudaError_t slab_pack(spns_handle *h, void *full, void *stage, int nf, int n1, int n2, const spns::SlabRanges &r, int axis,
+                                 int unpack) {
+        const long long n = (long long)nf * n1 * n2 * h->g.Kz;
+        const int blocks = (int)std::min<long long>((n + 255) / 256, 16LL * h->sms);
+        spns::k_slab_pack<T><<<blocks, 256, 0, h->st>>>((C *)full, (C *)stage, nf, n1, n2, h->g.Kz, r, axis, unpack);
+        return cudaGetLastError();
+    }
+    // Offsets of the staging blocks: block s holds nf * (axis 1: count_s * n2, axis 2: n1 * count_s) * Kz.
+    static spns::SlabRanges slab_offsets(const spns::SlabRanges &r0, int nf, int n1, int n2, int Kz, int axis) {
+        spns::SlabRanges r = r0;
+        long long o = 0;
+        for (int s = 0; s < r.n; s++) {
+            r.off[s] = o;
+            o += (long long)nf * (axis == 1 ? (long long)r.count[s] * n2 : (long long)n1 * r.count[s]) * Kz;
+        }
+        return r;
+    }
+    // The y and z passes run on this rank's x planes: swap the x-slab geometry and S1 buffer in.
+    static void slab_swap(spns_handle *h) {
+        std::swap(h->g, h->gx);
+        std::swap(h->B1, h->B1x);
+    }
+    // Phases of one step (advective arithmetic or LES; the caller exchanges the
+    // staging arrays and reduces the scalars between phases, see include/spns.h):
+    //   VEL_A  inverse x pass of u, v, w on this rank's ky rows; pack for the exchange
+    //   VEL_B  unpack; inverse y pass and z pass of u, v, w on this rank's x planes (CFL maxima)
+    //   DT     time step from the maxima reduced over the ranks
+    //   A      [forced shells' energy of this slab]; inverse x pass; pack
+    //   B      unpack; [forcing amplitude]; inverse y, z and forward y passes; pack back
+    //   C      unpack; forward x pass; spectral sweep; end of the step
+    static int slab_phase(spns_handle *h, int phase) {
+        const spns::Geo gy = h->g, gx = h->gx;
+        const int ny = gy.Ky, Mx = gy.Mx, Ky = gx.Ky, nx = gx.Mx, Kz = gy.Kz;
+        const bool les = h->a.isLES;
+        const int nf1 = spns::Fields<spns::MODE_ADV>::K1;                        // 6 (advective and LES)
+        const int nf4 = les ? spns::Fields<spns::MODE_LES>::K4 : spns::Fields<spns::MODE_ADV>::K4;
+        const spns::SlabRanges fwd_pack3 = slab_offsets(h->xr, 3, ny, Mx, Kz, 2), fwd_unpack3 = slab_offsets(h->yr, 3, Ky, nx, Kz, 1);
+        const spns::SlabRanges fwd_pack = slab_offsets(h->xr, nf1, ny, Mx, Kz, 2), fwd_unpack = slab_offsets(h->yr, nf1, Ky, nx, Kz, 1);
+        const spns::SlabRanges back_pack = slab_offsets(h->yr, nf4, Ky, nx, Kz, 1), back_unpack = slab_offsets(h->xr, nf4, ny, Mx, Kz, 2);
+        int r = SPNS_OK;
+        auto xpasses = [&](auto body) -> int {
+            slab_swap(h);
+            const int rr = body();
+            slab_swap(h);
+            return rr;
+        };
+        switch (phase) {
+        case SPNS_SLAB_VEL_A:
+            DISPATCH(gy.Mx, LAUNCH((launch_k1<LL, spns::MODE_VEL>(h))));
+            LAUNCH(slab_pack(h, h->B1, h->XS, 3, ny, Mx, fwd_pack3, 2, 0));
+            return SPNS_OK;
+        case SPNS_SLAB_VEL_B:
+            LAUNCH(slab_pack(h, h->B1x, h->XR, 3, Ky, nx, fwd_unpack3, 1, 1));
+            r = xpasses([&]() -> int {
+                spns::k_reset_max<<<1, 1, 0, h->st>>>(h->ds);
+                CKL();
+                DISPATCH(gx.My, LAUNCH((launch_k2<LL, spns::MODE_VEL>(h))));
+                DISPATCH(gx.Mz, LAUNCH((launch_k3<LL, spns::MODE_VEL>(h, nullptr))));
+                return SPNS_OK;
+            });
+            return r;
+        case SPNS_SLAB_DT:
+            spns::k_recalc_dt<<<1, 1, 0, h->st>>>(h->c, h->ds);
+            CKL();
+            return SPNS_OK;
+        case SPNS_SLAB_A:
+            if (h->a.eps_forcing > 0.0) {
+                spns::k_eps_band<T><<<1, spns::EPS_BAND_THREADS, 0, h->st>>>(gy, U(h, 0), U(h, 1), U(h, 2), Ulo(h, 0), Ulo(h, 1), Ulo(h, 2),
+                                                                          h->a.eps_kmin, h->a.eps_kmax, h->a.eps_forcing, h->ds, 1);
+                CKL();
+            }
+            if (les) { DISPATCH(gy.Mx, LAUNCH((launch_k1<LL, spns::MODE_LES>(h)))); }
+            else { DISPATCH(gy.Mx, LAUNCH((launch_k1<LL, spns::MODE_ADV>(h)))); }
+            LAUNCH(slab_pack(h, h->B1, h->XS, nf1, ny, Mx, fwd_pack, 2, 0));
+            return SPNS_OK;
+        case SPNS_SLAB_B:
+            LAUNCH(slab_pack(h, h->B1x, h->XR, nf1, Ky, nx, fwd_unpack, 1, 1));
+            if (h->a.eps_forcing > 0.0) {
+                spns::k_eps_alpha<<<1, 1, 0, h->st>>>(h->a.eps_forcing, h->ds);
+                CKL();
+            }
+            r = xpasses([&]() -> int {
+#define SLAB_YZ(MD)                                                                    \
+                DISPATCH(gx.My, LAUNCH((launch_k2<LL, MD>(h))));                      \
+                spns::k_reset_max<<<1, 1, 0, h->st>>>(h->ds);                          \
+                CKL();                                                                 \
+                DISPATCH(gx.Mz, LAUNCH((launch_k3<LL, MD>(h, nullptr))));             \
+                DISPATCH(gx.My, LAUNCH((launch_k4<LL, MD>(h))));
+                if (les) { SLAB_YZ(spns::MODE_LES) } else { SLAB_YZ(spns::MODE_ADV) }
+#undef SLAB_YZ
+                return SPNS_OK;
+            });
+            if (r) return r;
+            LAUNCH(slab_pack(h, h->B1x, h->XS, nf4, Ky, nx, back_pack, 1, 0));
+            return SPNS_OK;
+        case SPNS_SLAB_C:
+            LAUNCH(slab_pack(h, h->B1, h->XR, nf4, ny, Mx, back_unpack, 2, 1));
+            if (les) { DISPATCH(gy.Mx, LAUNCH((launch_k5<LL, spns::MODE_LES>(h)))); }
+            else { DISPATCH(gy.Mx, LAUNCH((launch_k5<LL, spns::MODE_ADV>(h)))); }
+            LAUNCH(launch_k6(h));
+            spns::k_finish_step<<<1, 1, 0, h->st>>>(h->c, h->ds);
+            CKL();
+            return SPNS_OK;
+        default:
+            return spns_fail(h, SPNS_ERR_INVALID_ARGUMENT, "unknown slab phase %d", phase);
+        }
+    }
+
     static constexpr PrecOps ops() {
-        return PrecOps{&step_once, &run_velocity, &shell_sums, &forcing_scale, &conj_correction, &seed_draw, &invariant_spectra};
+        return PrecOps{&step_once, &run_velocity, &shell_sums, &forcing_scale, &conj_correction, &seed_draw, &invariant_spectra,
+                       &slab_phase};
     }
 };

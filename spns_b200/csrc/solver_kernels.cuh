@@ -35,12 +35,19 @@ enum Mode { MODE_VEL = 0, MODE_ROT = 1, MODE_ADV = 2, MODE_LES = 3, MODE_INV = 4
 // on the grid and transforms them forward, the forward y/x passes carry 5 fields.
 
 struct Geo {
-    int Kx, Ky, Kz;   // retained mode counts
+    int Kx, Ky, Kz;   // retained mode counts (Ky: rows held, the slab's in a slab decomposition)
     int hx, hy, hz;   // half widths
-    int Mx, My, Mz;   // true FFT grid
+    int Mx, My, Mz;   // true FFT grid (Mx: x planes held, the slab's in the y/z passes of a slab decomposition)
     int sx, sy, sz;   // wavenumber scale per axis (length factor)
     long long S0, S1, S2; // elements per field in each layout
+    int y0, Kyg;      // first compact ky row held and the box's compact ky count (0 and Ky on one GPU)
 };
+
+// m2 (ky/sy) of compact row iy held by this geometry
+__host__ __device__ __forceinline__ int ky_mode(const Geo &g, int iy) {
+    const int r = g.y0 + iy;
+    return r <= g.hy ? r : r - g.Kyg;
+}
 
 // Solver scalars living in device memory (read by kernels, updated by the
 // finisher), so that a captured step stays valid while they change.
@@ -53,6 +60,7 @@ struct DevScalars {
     long long iter;
     int nonfinite, domain_err;
     int wait_timeout;                    // a bounded wait of a staged pass gave up (SPNS_ERR_TIMEOUT)
+    double ef;                           // slab decomposition: this slab's energy of the forced shells
 };
 
 struct StepConsts {
@@ -106,7 +114,7 @@ __global__ void __launch_bounds__(P *(L / E), AxisMinBlocks<T, 1>::N) k1_inv_x(G
     const int iy = blockIdx.y, kz = blockIdx.x * P + p;
     const bool ok = kz < g.Kz;
     const T kzf = T(g.sz * kz);
-    const T kyf = T(g.sy * (iy <= g.hy ? iy : iy - g.Ky));
+    const T kyf = T(g.sy * ky_mode(g, iy));
     SmRowMajor<T, P> sm{reinterpret_cast<cx<T> *>(smraw), p};
     const long long rb = (long long)iy * g.Kx;
 #pragma unroll 1
@@ -1021,7 +1029,7 @@ __global__ void __launch_bounds__(256) k6_sweep(Geo g, const cx<T> *__restrict__
             for (int i = 0; i < 3; i++) upl[i] = first ? ul[i] : Un1lo[i * S0 + idx];
         }
     }
-    const int m1 = ix <= g.hx ? ix : ix - g.Kx, m2 = iy <= g.hy ? iy : iy - g.Ky;
+    const int m1 = ix <= g.hx ? ix : ix - g.Kx, m2 = ky_mode(g, iy);
     const long long k1 = (long long)g.sx * m1, k2 = (long long)g.sy * m2, k3 = (long long)g.sz * kz;
     const double rad2 = (double)(k1 * k1 + k2 * k2 + k3 * k3);
     const bool mean = !(rad2 > 0.0);
@@ -1176,7 +1184,7 @@ __global__ void k_shell_sums(Geo g, const cx<T> *__restrict__ u, const cx<T> *__
         const long long t = idx / g.Kz;
         const int ix = (int)(t % g.Kx), iy = (int)(t / g.Kx);
         const long long k1 = (long long)g.sx * (ix <= g.hx ? ix : ix - g.Kx);
-        const long long k2 = (long long)g.sy * (iy <= g.hy ? iy : iy - g.Ky);
+        const long long k2 = (long long)g.sy * ky_mode(g, iy);
         const long long k3 = (long long)g.sz * kz;
         const double rad2 = (double)(k1 * k1 + k2 * k2 + k3 * k3);
         const int K = (int)round(sqrt(rad2));
@@ -1208,7 +1216,7 @@ __global__ void k_shell_sums_scalar(Geo g, const cx<T> *__restrict__ F, double s
         const long long t = idx / g.Kz;
         const int ix = (int)(t % g.Kx), iy = (int)(t / g.Kx);
         const long long k1 = (long long)g.sx * (ix <= g.hx ? ix : ix - g.Kx);
-        const long long k2 = (long long)g.sy * (iy <= g.hy ? iy : iy - g.Ky);
+        const long long k2 = (long long)g.sy * ky_mode(g, iy);
         const long long k3 = (long long)g.sz * kz;
         const int K = (int)round(sqrt((double)(k1 * k1 + k2 * k2 + k3 * k3)));
         if (K > Kmax) continue;
@@ -1243,11 +1251,13 @@ static __global__ void k_totals(const double *Ek, const double *Om, int Kmax, De
 // so one block visits that sub-box directly, in a fixed order with a fixed
 // reduction tree: alpha does not depend on timing.  EPS_BAND_THREADS threads.
 constexpr int EPS_BAND_THREADS = 256;
+// partial (slab decomposition): only the rows this geometry holds are summed and the
+// sum goes to ds->ef, for the caller to add up over the slabs and k_eps_alpha to use.
 template <typename T>
 __global__ void __launch_bounds__(EPS_BAND_THREADS) k_eps_band(Geo g, const cx<T> *__restrict__ u, const cx<T> *__restrict__ v,
                                                                const cx<T> *__restrict__ w, const cx<T> *__restrict__ ulo,
                                                                const cx<T> *__restrict__ vlo, const cx<T> *__restrict__ wlo,
-                                                               int kmin, int kmax, double eps, DevScalars *ds) {
+                                                               int kmin, int kmax, double eps, DevScalars *ds, int partial = 0) {
     __shared__ double red[EPS_BAND_THREADS];
     const int mx = min(g.hx, (kmax + 1) / g.sx), my = min(g.hy, (kmax + 1) / g.sy), mz = min(g.hz, (kmax + 1) / g.sz);
     const int nx = 2 * mx + 1, ny = 2 * my + 1, nz = mz + 1;
@@ -1256,7 +1266,8 @@ __global__ void __launch_bounds__(EPS_BAND_THREADS) k_eps_band(Geo g, const cx<T
     for (int c = threadIdx.x; c < count; c += EPS_BAND_THREADS) {
         const int kz = c % nz, t = c / nz;
         const int m1 = t % nx - mx, m2 = t / nx - my;
-        const int ix = m1 >= 0 ? m1 : m1 + g.Kx, iy = m2 >= 0 ? m2 : m2 + g.Ky;
+        const int ix = m1 >= 0 ? m1 : m1 + g.Kx, iy = (m2 >= 0 ? m2 : m2 + g.Kyg) - g.y0;
+        if (iy < 0 || iy >= g.Ky) continue;   // row held by another slab
         const long long k1 = (long long)g.sx * m1, k2 = (long long)g.sy * m2, k3 = (long long)g.sz * kz;
         const int K = (int)round(sqrt((double)(k1 * k1 + k2 * k2 + k3 * k3)));
         if (K < kmin || K > kmax) continue;
@@ -1274,8 +1285,15 @@ __global__ void __launch_bounds__(EPS_BAND_THREADS) k_eps_band(Geo g, const cx<T
     }
     if (threadIdx.x == 0) {
         const double Ef = red[0];
-        ds->alpha = Ef > 1e-30 ? eps / (2.0 * Ef) : 0.0;
+        if (partial) ds->ef = Ef;
+        else ds->alpha = Ef > 1e-30 ? eps / (2.0 * Ef) : 0.0;
     }
+}
+
+// alpha from the forced shells' energy summed over the slabs (ds->ef)
+static __global__ void k_eps_alpha(double eps, DevScalars *ds) {
+    const double Ef = ds->ef;
+    ds->alpha = Ef > 1e-30 ? eps / (2.0 * Ef) : 0.0;
 }
 
 
@@ -1296,7 +1314,7 @@ __global__ void k_forcing_scale(Geo g, cx<T> *u, cx<T> *v, cx<T> *w, cx<T> *ulo,
         const long long t = idx / g.Kz;
         const int ix = (int)(t % g.Kx), iy = (int)(t / g.Kx);
         const long long k1 = (long long)g.sx * (ix <= g.hx ? ix : ix - g.Kx);
-        const long long k2 = (long long)g.sy * (iy <= g.hy ? iy : iy - g.Ky);
+        const long long k2 = (long long)g.sy * ky_mode(g, iy);
         const long long k3 = (long long)g.sz * kz;
         const int K = (int)round(sqrt((double)(k1 * k1 + k2 * k2 + k3 * k3)));
         if (K <= last_eff) {
@@ -1334,6 +1352,39 @@ __global__ void k_conj_correction(Geo g, cx<T> *u, cx<T> *v, cx<T> *w, cx<T> *ul
             u[dst] = conj(u[src]); v[dst] = conj(v[src]); w[dst] = conj(w[src]);
             if (ulo) { ulo[dst] = conj(ulo[src]); vlo[dst] = conj(vlo[src]); wlo[dst] = conj(wlo[src]); }
         }
+    }
+}
+
+// ===========================================================================
+// Slab decomposition: reorder of a [nf][n1][n2][Kz] array into per-rank blocks
+// [s][f][n1_s][n2_s][Kz] split along axis 1 (rows n1) or 2 (n2) by the ranks'
+// block ranges (FFTW-MPI's default block: ceil(n/ranks) per rank), and back.
+// Block s starts at off[s] of the staging array; a rank's outgoing blocks are
+// contiguous there, in rank order, as an all-to-all sends them.
+// ===========================================================================
+#define SPNS_SLAB_MAX_RANKS 64
+struct SlabRanges {
+    int n, blk;                          // ranks, block size of the split axis
+    int start[SPNS_SLAB_MAX_RANKS], count[SPNS_SLAB_MAX_RANKS];
+    long long off[SPNS_SLAB_MAX_RANKS];  // element offset of rank s's block in the staging array
+};
+template <typename T>
+__global__ void k_slab_pack(cx<T> *__restrict__ full, cx<T> *__restrict__ stage, int nf, int n1, int n2, int Kz, SlabRanges r, int axis,
+                            int unpack) {
+    const long long n = (long long)nf * n1 * n2 * Kz;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long long)gridDim.x * blockDim.x) {
+        const int kz = (int)(idx % Kz);
+        long long t = idx / Kz;
+        const int i2 = (int)(t % n2);
+        t /= n2;
+        const int i1 = (int)(t % n1), f = (int)(t / n1);
+        const int a = axis == 1 ? i1 : i2;
+        const int s = a / r.blk;
+        const int loc = a - r.start[s];
+        const int n1s = axis == 1 ? r.count[s] : n1, n2s = axis == 1 ? n2 : r.count[s];
+        const long long st = r.off[s] + (((long long)f * n1s + (axis == 1 ? loc : i1)) * n2s + (axis == 1 ? i2 : loc)) * Kz + kz;
+        if (unpack) full[idx] = stage[st];
+        else stage[st] = full[idx];
     }
 }
 

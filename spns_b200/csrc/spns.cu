@@ -278,6 +278,8 @@ static int box_geometry(const spns_hit_args &a, Geo &g, int &last_rad, int &last
     g.S0 = (long long)g.Ky * g.Kx * g.Kz;
     g.S1 = (long long)g.Ky * g.Mx * g.Kz;
     g.S2 = (long long)g.My * g.Mx * g.Kz;
+    g.y0 = 0;
+    g.Kyg = g.Ky;
     if (!spns_length_supported(g.Mx) || !spns_length_supported(g.My) || !spns_length_supported(g.Mz))
         return spns_fail(nullptr, SPNS_ERR_UNSUPPORTED_SIZE, "FFT grid %dx%dx%d outside the compiled lengths", g.Mx, g.My, g.Mz);
     if (2 * g.hx >= g.Mx || 2 * g.hy >= g.My || 2 * g.hz >= g.Mz)
@@ -285,6 +287,36 @@ static int box_geometry(const spns_hit_args &a, Geo &g, int &last_rad, int &last
     last_rad = std::min((a.Nx - 1) / 2, std::min((a.Ny - 1) / 2, (a.Nz - 1) / 2));
     last_rad_max = (int)std::ceil(std::sqrt(1.0 * (a.Nx / 2) * (a.Nx / 2) + 1.0 * (a.Ny / 2) * (a.Ny / 2) + 1.0 * (a.Nz / 2) * (a.Nz / 2)));
     return SPNS_OK;
+}
+
+// Step constants of a box (src/HIT_LES.h:31-58, src/HIT_LES.cpp:1049-1078 for the
+// self-adaptive scheme) from the geometry of the whole box.
+static void step_consts(spns_handle *h, const Geo &g) {
+    const spns_hit_args &a = h->a;
+    const int AMx = g.Mx, AMy = g.My, AMz = g.Mz;
+    const double PI_ = 3.141592653589793238462643;
+    StepConsts &c = h->c;
+    memset(&c, 0, sizeof(c));
+    c.inv_norm = 1.0 / ((double)g.Mx * g.My * g.Mz);
+    c.omega_x = a.omega_x; c.omega_y = a.omega_y; c.omega_z = a.omega_z;
+    c.Ax = 2.0 * PI_ / AMx / a.Lx_factor; c.Ay = 2.0 * PI_ / AMy / a.Ly_factor; c.Az = 2.0 * PI_ / AMz / a.Lz_factor;
+    c.inv_Ax = 1.0 / c.Ax; c.inv_Ay = 1.0 / c.Ay; c.inv_Az = 1.0 / c.Az;
+    c.C_At = a.C_At;
+    h->delta = 2.0 * PI_ / std::cbrt((double)((long long)a.Lx_factor * a.Ly_factor * a.Lz_factor * AMx * AMy * AMz));
+    c.les_ct = a.C_Smag * a.C_Smag * h->delta * h->delta;
+    c.fixed_dt = a.fixed_dt;
+    c.eps_on = a.eps_forcing > 0.0;
+    c.eps_kmin = a.eps_kmin; c.eps_kmax = a.eps_kmax;
+    c.rotating = a.isRotating;
+    c.self_adaptive = a.isSelfAdaptive;
+    // self-adaptive constants (src/HIT_LES.cpp:1049-1078)
+    c.Ah = (c.Ax + c.Ay + c.Az) / 3.0;
+    c.t1 = 0.9302468;
+    c.kopt_k[0] = 0.73782212; c.kopt_k[1] = 0.44660387;
+    c.phi[0] = std::atan(164.0 / 99.0); c.phi[1] = PI_ / 3.0; c.phi[2] = PI_ * 3.0 * 3.0 / (5.0 * 5.0);
+    const double cc[14] = {0.0647998, -0.386022, 3.72945, -9.38143, 7.06574, 2403400.0, -5018490.0,
+                           2620140.0, 2945.0, -6665.76, 3790.54, 4.80513, -16.9473, 15.0155};
+    memcpy(c.c, cc, sizeof(cc));
 }
 
 // Device buffers of a handle (bytes), in the order spns_create allocates them.
@@ -327,7 +359,7 @@ static void free_handle(spns_handle *h) {
     // stream-ordered frees: no device-wide synchronisation, so other handles'
     // work in flight (a serving loop) keeps running while this one is released
     void *bufs[] = {h->ds, h->U, h->Ulo, h->R, h->Up, h->Uplo, h->B1, h->B2, h->bins, h->FT, h->forced, h->phys, h->edge,
-                    h->inv_B1, h->inv_B2, h->inv_bins};
+                    h->inv_B1, h->inv_B2, h->inv_bins, h->B1x, h->XS, h->XR};
     for (void *b : bufs)
         if (b) cudaFreeAsync(b, h->st);
     for (auto &kv : h->tw) cudaFreeAsync(kv.second, h->st);
@@ -380,32 +412,9 @@ int spns_create(const spns_hit_args *args, const double *file_uvw, spns_handle *
     }
     h->g = g0;
     const Geo &g = h->g;
-    const int AMx = g.Mx, AMy = g.My, AMz = g.Mz;
     h->last_rad = last_rad;
     h->last_rad_max = last_rad_max;
-    const double PI_ = 3.141592653589793238462643;
-    StepConsts &c = h->c;
-    memset(&c, 0, sizeof(c));
-    c.inv_norm = 1.0 / ((double)g.Mx * g.My * g.Mz);
-    c.omega_x = a.omega_x; c.omega_y = a.omega_y; c.omega_z = a.omega_z;
-    c.Ax = 2.0 * PI_ / AMx / a.Lx_factor; c.Ay = 2.0 * PI_ / AMy / a.Ly_factor; c.Az = 2.0 * PI_ / AMz / a.Lz_factor;
-    c.inv_Ax = 1.0 / c.Ax; c.inv_Ay = 1.0 / c.Ay; c.inv_Az = 1.0 / c.Az;
-    c.C_At = a.C_At;
-    h->delta = 2.0 * PI_ / std::cbrt((double)((long long)a.Lx_factor * a.Ly_factor * a.Lz_factor * AMx * AMy * AMz));
-    c.les_ct = a.C_Smag * a.C_Smag * h->delta * h->delta;
-    c.fixed_dt = a.fixed_dt;
-    c.eps_on = a.eps_forcing > 0.0;
-    c.eps_kmin = a.eps_kmin; c.eps_kmax = a.eps_kmax;
-    c.rotating = a.isRotating;
-    c.self_adaptive = a.isSelfAdaptive;
-    // self-adaptive constants (src/HIT_LES.cpp:1049-1078)
-    c.Ah = (c.Ax + c.Ay + c.Az) / 3.0;
-    c.t1 = 0.9302468;
-    c.kopt_k[0] = 0.73782212; c.kopt_k[1] = 0.44660387;
-    c.phi[0] = std::atan(164.0 / 99.0); c.phi[1] = PI_ / 3.0; c.phi[2] = PI_ * 3.0 * 3.0 / (5.0 * 5.0);
-    const double cc[14] = {0.0647998, -0.386022, 3.72945, -9.38143, 7.06574, 2403400.0, -5018490.0,
-                           2620140.0, 2945.0, -6665.76, 3790.54, 4.80513, -16.9473, 15.0155};
-    memcpy(c.c, cc, sizeof(cc));
+    step_consts(h, g);
 
     // device memory
     auto cleanup = [&](int code) { free_handle(h); return code; };
@@ -892,6 +901,7 @@ int spns_seed_field(spns_handle *h, uint64_t seed, double kp, double urms) {
 // no status check); spns_synchronize completes them.
 int spns_step_async(spns_handle *h, int nsteps) {
     if (!h || nsteps < 0) return SPNS_ERR_INVALID_ARGUMENT;
+    if (h->slab_ranks > 0) return spns_fail(h, SPNS_ERR_INVALID_ARGUMENT, "a slab handle steps through spns_slab_phase");
     for (int i = 0; i < nsteps; i++) {
         const bool profiling = h->prof_steps < h->prof_cap_steps;
         const bool warm = h->kernels_per_step > 0;   // a first step has run uncaptured
@@ -991,6 +1001,186 @@ int spns_checkpoint_load(spns_handle *h, const void *buf, size_t bytes) {
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------
+// Slab decomposition of one box over several GPUs (see include/spns.h)
+// ---------------------------------------------------------------------------
+extern "C" int spns_slab_block(int n, int nranks, int rank, int *start, int *count) {
+    if (n < 1 || nranks < 1 || rank < 0 || rank >= nranks || !start || !count) return SPNS_ERR_INVALID_ARGUMENT;
+    const int blk = (n + nranks - 1) / nranks;
+    const int s0 = std::min(n, rank * blk);
+    *start = s0;
+    *count = std::min(n, s0 + blk) - s0;
+    return SPNS_OK;
+}
+
+static bool slab_ranges(int n, int nranks, SlabRanges &r) {
+    memset(&r, 0, sizeof(r));
+    r.n = nranks;
+    r.blk = (n + nranks - 1) / nranks;
+    for (int s = 0; s < nranks; s++) {
+        spns_slab_block(n, nranks, s, &r.start[s], &r.count[s]);
+        if (r.count[s] < 1) return false;
+    }
+    return true;
+}
+
+extern "C" int spns_slab_create(const spns_hit_args *args, int nranks, int rank, spns_handle **out) {
+    if (!args || !out) return spns_fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    if (nranks < 1 || nranks > SPNS_SLAB_MAX_RANKS || rank < 0 || rank >= nranks)
+        return spns_fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "rank %d of %d outside 1..%d ranks", rank, nranks, SPNS_SLAB_MAX_RANKS);
+    if (!args->isLES && args->nonlinear_form != 2)
+        return spns_fail(nullptr, SPNS_ERR_INVALID_ARGUMENT, "a slab decomposition runs the advective form (nonlinear_form 2) or LES");
+    if (args->isComplexConjugateCorrected || args->isReLambda || args->isInitialFieldFromFile)
+        return spns_fail(nullptr, SPNS_ERR_INVALID_ARGUMENT,
+                         "conjugate correction, Re_lambda forcing and file initial fields are not available on slabs");
+    Geo gf;
+    int last_rad = 0, last_rad_max = 0;
+    int rc = box_geometry(*args, gf, last_rad, last_rad_max);
+    if (rc) return rc;
+    SlabRanges yr, xr;
+    if (!slab_ranges(gf.Ky, nranks, yr) || !slab_ranges(gf.Mx, nranks, xr))
+        return spns_fail(nullptr, SPNS_ERR_UNSUPPORTED_SIZE, "%d ranks leave a rank without ky rows (%d) or x planes (%d)", nranks, gf.Ky,
+                         gf.Mx);
+    spns_handle *h = new spns_handle();
+    h->a = *args;
+    h->a.isInitialFieldFromFile = 0;
+    h->prec = args->precision;
+    h->csz = h->prec == SPNS_FP64 ? sizeof(double2) : sizeof(float2);
+    const spns_hit_args &a = h->a;
+    if (cudaSetDevice(a.device) != cudaSuccess) { delete h; return spns_fail(nullptr, SPNS_ERR_CUDA, "cudaSetDevice(%d) failed", a.device); }
+    h->slab_ranks = nranks;
+    h->slab_rank = rank;
+    h->yr = yr;
+    h->xr = xr;
+    h->x0 = xr.start[rank];
+    h->last_rad = last_rad;
+    h->last_rad_max = last_rad_max;
+    // this rank's ky rows (state, x passes, sweep) and x planes (y and z passes)
+    Geo g = gf;
+    g.Ky = yr.count[rank];
+    g.y0 = yr.start[rank];
+    g.Kyg = gf.Ky;
+    g.S0 = (long long)g.Ky * g.Kx * g.Kz;
+    g.S1 = (long long)g.Ky * g.Mx * g.Kz;
+    g.S2 = 0;
+    Geo gx = gf;
+    gx.Mx = xr.count[rank];
+    gx.S0 = 0;
+    gx.S1 = (long long)gf.Ky * gx.Mx * gf.Kz;
+    gx.S2 = (long long)gf.My * gx.Mx * gf.Kz;
+    h->g = g;
+    h->gx = gx;
+    step_consts(h, gf);
+    auto cleanup = [&](int code) { free_handle(h); return code; };
+    {
+        int least = 0, greatest = 0;
+        cudaDeviceGetStreamPriorityRange(&least, &greatest);
+        const int prio = std::max(greatest, std::min(least, a.stream_priority));
+        int dev = 0;
+        if (cudaStreamCreateWithPriority(&h->st, cudaStreamNonBlocking, prio) != cudaSuccess || cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || h->sms < 1)
+            return cleanup(spns_fail(nullptr, SPNS_ERR_CUDA, "stream creation failed"));
+    }
+    const size_t cs = h->csz;
+    const bool hilo = h->prec == SPNS_FP32_HILO;
+    const size_t state = cs * 3 * (size_t)g.S0;
+    h->nB1 = 6;
+    h->nB2 = 9;
+    h->xelems = 6 * (size_t)std::max(g.S1, gx.S1);
+    auto amalloc = [&](void **p, size_t n) { return n == 0 || cudaMallocAsync(p, n, h->st) == cudaSuccess; };
+    const bool okm = amalloc((void **)&h->ds, sizeof(DevScalars)) && amalloc(&h->U, state) && amalloc(&h->Ulo, hilo ? state : 0) &&
+                     amalloc(&h->R, state) && amalloc(&h->Up, a.isSelfAdaptive ? state : 0) &&
+                     amalloc(&h->Uplo, a.isSelfAdaptive && hilo ? state : 0) && amalloc(&h->B1, cs * 6 * (size_t)g.S1) &&
+                     amalloc(&h->B1x, cs * 6 * (size_t)gx.S1) &&
+                     amalloc(&h->B2, cs * std::max(9 * (size_t)gx.S2, 3 * (size_t)g.S0)) &&
+                     amalloc((void **)&h->bins, sizeof(double) * 2 * (size_t)(last_rad_max + 1)) && amalloc(&h->XS, cs * h->xelems) &&
+                     amalloc(&h->XR, cs * h->xelems);
+    if (!okm) { cudaGetLastError(); return cleanup(spns_fail(nullptr, SPNS_ERR_OUT_OF_MEMORY, "device allocation failed")); }
+    for (int L : {gf.Mx, gf.My, gf.Mz})
+        if (!h->tw.count(L)) {
+            void *t = hilo ? spns_make_twiddles<float>(L, h->st) : spns_make_twiddles<double>(L, h->st);
+            if (!t) return cleanup(spns_fail(nullptr, SPNS_ERR_OUT_OF_MEMORY, "twiddle allocation failed"));
+            h->tw[L] = t;
+        }
+    DevScalars s0v;
+    memset(&s0v, 0, sizeof(s0v));
+    s0v.nu = a.nu;
+    s0v.kappa = 0.5;
+    const bool okz = cudaMemsetAsync(h->U, 0, state, h->st) == cudaSuccess && (!h->Ulo || cudaMemsetAsync(h->Ulo, 0, state, h->st) == cudaSuccess) &&
+                     cudaMemsetAsync(h->R, 0, state, h->st) == cudaSuccess && (!h->Up || cudaMemsetAsync(h->Up, 0, state, h->st) == cudaSuccess) &&
+                     (!h->Uplo || cudaMemsetAsync(h->Uplo, 0, state, h->st) == cudaSuccess) &&
+                     cudaMemcpyAsync(h->ds, &s0v, sizeof(s0v), cudaMemcpyHostToDevice, h->st) == cudaSuccess &&
+                     cudaStreamSynchronize(h->st) == cudaSuccess;
+    if (!okz) return cleanup(spns_fail(nullptr, SPNS_ERR_CUDA, "buffer initialisation failed"));
+    h->U0 = h->U;
+    h->use_graphs = false;
+    *out = h;
+    return SPNS_OK;
+}
+
+extern "C" int spns_slab_layout(spns_handle *h, int *y0, int *ny, int *x0, int *nx) {
+    if (!h || h->slab_ranks < 1) return SPNS_ERR_INVALID_ARGUMENT;
+    if (y0) *y0 = h->g.y0;
+    if (ny) *ny = h->g.Ky;
+    if (x0) *x0 = h->x0;
+    if (nx) *nx = h->gx.Mx;
+    return SPNS_OK;
+}
+
+extern "C" int spns_slab_phase(spns_handle *h, int phase) {
+    if (!h || h->slab_ranks < 1) return SPNS_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(h->a.device);
+    const int r = spns_ops(h).slab_phase(h, phase);
+    if (r) return r;
+    return phase == SPNS_SLAB_C ? check_flags(h) : SPNS_OK;
+}
+
+extern "C" int spns_slab_counts(int Ky, int Mx, int Kz, int nranks, int rank, int nf, int back, long long *send, long long *recv) {
+    if (Ky < 1 || Mx < 1 || Kz < 1 || nf < 1 || nranks < 1 || rank < 0 || rank >= nranks || !send || !recv)
+        return SPNS_ERR_INVALID_ARGUMENT;
+    int y0m, nym, x0m, nxm;
+    spns_slab_block(Ky, nranks, rank, &y0m, &nym);
+    spns_slab_block(Mx, nranks, rank, &x0m, &nxm);
+    for (int s = 0; s < nranks; s++) {
+        int y0s, nys, x0s, nxs;
+        spns_slab_block(Ky, nranks, s, &y0s, &nys);
+        spns_slab_block(Mx, nranks, s, &x0s, &nxs);
+        if (!back) {   // ky rows -> x planes: to s goes [f][my rows][s's planes]
+            send[s] = (long long)nf * nym * nxs * Kz;
+            recv[s] = (long long)nf * nys * nxm * Kz;
+        } else {       // x planes -> ky rows: to s goes [f][s's rows][my planes]
+            send[s] = (long long)nf * nys * nxm * Kz;
+            recv[s] = (long long)nf * nym * nxs * Kz;
+        }
+    }
+    return SPNS_OK;
+}
+
+extern "C" int spns_slab_exchange(spns_handle *h, int phase, long long *send, long long *recv) {
+    if (!h || h->slab_ranks < 1 || !send || !recv) return SPNS_ERR_INVALID_ARGUMENT;
+    const int Ky = h->gx.Ky, Mx = h->g.Mx, Kz = h->g.Kz;
+    const int nf4 = h->a.isLES ? spns::Fields<spns::MODE_LES>::K4 : spns::Fields<spns::MODE_ADV>::K4;
+    if (phase == SPNS_SLAB_VEL_A) return spns_slab_counts(Ky, Mx, Kz, h->slab_ranks, h->slab_rank, 3, 0, send, recv);
+    if (phase == SPNS_SLAB_A) return spns_slab_counts(Ky, Mx, Kz, h->slab_ranks, h->slab_rank, 6, 0, send, recv);
+    if (phase == SPNS_SLAB_B) return spns_slab_counts(Ky, Mx, Kz, h->slab_ranks, h->slab_rank, nf4, 1, send, recv);
+    return spns_fail(h, SPNS_ERR_INVALID_ARGUMENT, "phase %d has no exchange", phase);
+}
+
+extern "C" int spns_slab_buffers(spns_handle *h, void **send, void **recv, size_t *elems, void **scalars, size_t *off) {
+    if (!h || h->slab_ranks < 1) return SPNS_ERR_INVALID_ARGUMENT;
+    if (send) *send = h->XS;
+    if (recv) *recv = h->XR;
+    if (elems) *elems = h->xelems;
+    if (scalars) *scalars = h->ds;
+    if (off) {
+        off[0] = offsetof(DevScalars, max_bits);
+        off[1] = offsetof(DevScalars, nonfinite);
+        off[2] = offsetof(DevScalars, ef);
+    }
+    return SPNS_OK;
+}
 
 // ---------------------------------------------------------------------------
 // Ensembles: one CUDA graph advances every member by one step.  Each member's

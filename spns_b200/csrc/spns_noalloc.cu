@@ -98,6 +98,8 @@ extern "C" int spns_energy_cascade_noalloc_f64(const void *uvw_dev, int Kx, int 
     g.hx = (Kx - 1) / 2; g.hy = (Ky - 1) / 2; g.hz = Kz - 1;
     g.sx = Lx_factor; g.sy = Ly_factor; g.sz = Lz_factor;
     g.S0 = (long long)Kx * Ky * Kz;
+    g.y0 = 0;
+    g.Kyg = Ky;
     const double2 *u = static_cast<const double2 *>(uvw_dev);
 
     // The array keeps the previous call's sums: clear the bins used here.

@@ -34,6 +34,8 @@ EXPORTED_SYMBOLS = (
     "spns_query", "spns_synchronize", "spns_checkpoint_bytes", "spns_checkpoint_save", "spns_checkpoint_load",
     "spns_ensemble_create", "spns_ensemble_step", "spns_ensemble_destroy", "spns_ensemble_last_error",
     "spns_invariant_spectra", "spns_eddy_viscosity_stats", "spns_autotune", "spns_autotune_forget", "spns_set_shapes",
+    "spns_slab_block", "spns_slab_create", "spns_slab_layout", "spns_slab_phase", "spns_slab_exchange", "spns_slab_counts",
+    "spns_slab_buffers",
 )
 
 
@@ -141,6 +143,14 @@ def lib():
         L.spns_autotune.argtypes = [vp, i, ip]
         L.spns_autotune_forget.argtypes = []
         L.spns_set_shapes.argtypes = [vp, ip]
+        lp = C.POINTER(C.c_longlong)
+        L.spns_slab_block.argtypes = [i, i, i, ip, ip]
+        L.spns_slab_create.argtypes = [C.POINTER(HitArgsC), i, i, C.POINTER(vp)]
+        L.spns_slab_layout.argtypes = [vp, ip, ip, ip, ip]
+        L.spns_slab_phase.argtypes = [vp, i]
+        L.spns_slab_exchange.argtypes = [vp, i, lp, lp]
+        L.spns_slab_counts.argtypes = [i, i, i, i, i, i, i, lp, lp]
+        L.spns_slab_buffers.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(sz), C.POINTER(vp), C.POINTER(sz)]
         _lib = L
     return _lib
 
