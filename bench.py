@@ -243,6 +243,39 @@ def fp32_accuracy_block(a, local: int, rank: int, steps: int):
             "shells_compared": "shells holding more than 1e-6 of the peak shell energy"}
 
 
+def stretch_block(local: int, n: int = 1024, steps: int = 5):
+    """The 1024^3 stretch of the forced DNS (FFT 1536^3) in the compensated FP32 form, which
+    fits one B200 (about 162 GB; the FP64 form needs about 272 GB and runs as slabs over
+    several GPUs).  Same workload as the headline box at N=1024."""
+    from spns_b200.hit import HIT, SPNS_FP32_HILO, SpnsError, estimate_device_bytes
+    import torch
+    a = box_args(n)
+    a.nu = nu_for(n)
+    out = {"N": n, "fft_grid": (3 * n) // 2, "precision": "FP32 compensated form",
+           "device_bytes": estimate_device_bytes(a, precision=SPNS_FP32_HILO, eps_forcing=EPS)}
+    try:
+        h = HIT(a, device=local, eps_forcing=EPS, precision=SPNS_FP32_HILO, k41_ranks=-1)
+    except SpnsError as e:
+        out["unavailable"] = str(e)
+        return out
+    h.seed_field(SEED, KP, 1.0)
+    h.New_Fractional_Step_Method(3)
+    stream = torch.cuda.ExternalStream(h.stream_handle(), device=torch.device("cuda", local))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    h._ck(h._L.spns_step(h._h, steps))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    energy = h.Recalculate_Energy()
+    s = h.scalars()
+    h.close()
+    out.update({"steps": steps, "ms_per_step": ms, "steps_per_s": 1e3 / ms, "energy": energy,
+                "finite": math.isfinite(s.At) and math.isfinite(energy)})
+    return out
+
+
 def same_n_block(local: int, n: int, threads: int, cpu_steps: int = 3, gpu_steps: int = 50):
     """The oracle and the GPU on the SAME forced-DNS box at a size the host can hold
     (N=n retained modes, FFT (3n/2)^3): measured steps/s of both, no extrapolation."""
@@ -295,7 +328,7 @@ def ensemble_block(local: int, n_boxes: int = 64, steps: int = 500, seed: int = 
              for _ in range(n_boxes)]
     members, shapes = [], {}
     for N, cs, sd in specs:
-        h = HIT(sbox(N, nu=1e-4, C_Smag=cs), precision=SPNS_FP32_HILO, device=local)
+        h = HIT(sbox(N, nu=1e-4, C_Smag=cs), precision=SPNS_FP32_HILO, device=local, k41_ranks=-1)
         h.seed_field(sd, 3.0, 1.0)
         shapes[str(N)] = h.autotune(steps=3)      # timed once per box class, then cached
         members.append(h)
@@ -312,7 +345,7 @@ def ensemble_block(local: int, n_boxes: int = 64, steps: int = 500, seed: int = 
     for prec, name in ((SPNS_FP32_HILO, "fp32_hilo"), (SPNS_FP64, "fp64")):
         tot = 0.0
         for N, cs, sd in specs:
-            h = HIT(sbox(N, nu=1e-4, C_Smag=cs), precision=prec, device=local)
+            h = HIT(sbox(N, nu=1e-4, C_Smag=cs), precision=prec, device=local, k41_ranks=-1)
             h.seed_field(sd, 3.0, 1.0)
             h.New_Fractional_Step_Method(3)
             tot += _timed_steps(h, probe) / probe * steps
@@ -349,7 +382,7 @@ def les_config_block(local: int, steps: int = 2000):
                 isNotCubic=True, isRotating=True, isLES=True, isComplexConjugateCorrected=False, isSelfAdaptive=False)
     runs, rate, probe = {}, {}, 50
     for prec in (SPNS_FP64, SPNS_FP32_HILO):
-        h = HIT(a, precision=prec, device=local)
+        h = HIT(a, precision=prec, device=local, k41_ranks=-1)
         h.seed_field(3, 3.0, 1.0)
         h.New_Fractional_Step_Method(3)
         rate[prec] = probe / _timed_steps(h, probe)
@@ -395,7 +428,7 @@ def serving_block(local: int, n_requests: int = 40, rate: float = 20.0, seed: in
         key = (r.args.Nx, r.args.isLES)
         if key in per_step:
             continue
-        h = HIT(r.args, precision=SPNS_FP64, device=local)
+        h = HIT(r.args, precision=SPNS_FP64, device=local, k41_ranks=-1)
         h.seed_field(r.seed, r.kp, r.urms)
         h.New_Fractional_Step_Method(3)
         per_step[key] = _timed_steps(h, probe) / probe
@@ -591,6 +624,8 @@ def run_gpu(args):
         line["ensemble"] = ensemble_block(local)
     if not args.no_serving:
         line["serving"] = serving_block(local, n_requests=args.serving_requests)
+    if not args.no_stretch:
+        line["stretch_n1024_fp32"] = stretch_block(local)
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_block(os.cpu_count() or 1)
         if args.same_n:
@@ -623,6 +658,7 @@ def main():
     ap.add_argument("--no-serving", action="store_true", help="skip the served-workload field")
     ap.add_argument("--no-les", action="store_true", help="skip the LES-configuration field (FP32 vs FP64)")
     ap.add_argument("--serving-requests", type=int, default=40)
+    ap.add_argument("--no-stretch", action="store_true", help="skip the 1024^3 FP32 stretch field")
     ap.add_argument("--accuracy-steps", type=int, default=100,
                     help="steps of the FP32-vs-FP64 accuracy comparison (0 skips it)")
     ap.add_argument("--same-n", type=int, default=128,

@@ -53,7 +53,9 @@ typedef struct spns_hit_args {
     /* extensions */
     int precision;           /* spns_precision                                          */
     int device;              /* CUDA device ordinal                                     */
-    int k41_ranks;           /* K41 initial field as generated by this many MPI ranks (>=1) */
+    int k41_ranks;           /* K41 initial field as generated by this many MPI ranks (>=1); a negative
+                                value starts from a zero state instead, for callers that set the state
+                                themselves (spns_set_spectral, spns_seed_field, spns_checkpoint_load) */
     double fixed_dt;         /* >0: constant time step instead of the CFL/self-adaptive one */
     double eps_forcing;      /* >0: constant-power forcing on shells [eps_kmin, eps_kmax]   */
     int eps_kmin, eps_kmax;  /*     (the disabled block src/HIT_LES.cpp:243-278, eps_in=eps) */

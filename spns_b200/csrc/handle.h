@@ -55,6 +55,12 @@ template <typename T, int L, int E_, int THR> struct ShapeT {
 #ifndef SPNS_K5_E
 #define SPNS_K5_E 24          // double forward x pass: complex values per thread
 #endif
+#ifndef SPNS_K5_T
+#define SPNS_K5_T 128         // double forward x pass: threads per block
+#endif
+#ifndef SPNS_K1_T
+#define SPNS_K1_T 256         // double inverse x pass: threads per block
+#endif
 #ifndef SPNS_K2_E
 #define SPNS_K2_E 24          // double y passes: complex values per thread
 #endif
@@ -99,9 +105,9 @@ template <typename T, int L, int E_, int THR> struct ShapeT {
 #endif
 template <typename T> struct ShapeSel {
     static constexpr bool D = sizeof(T) == 8;
-    static constexpr int K1_E = D ? SPNS_K1_E : SPNS_F32_K1_E, K1_T = D ? 256 : SPNS_F32_K1_T;
+    static constexpr int K1_E = D ? SPNS_K1_E : SPNS_F32_K1_E, K1_T = D ? SPNS_K1_T : SPNS_F32_K1_T;
     static constexpr int K2_E = D ? SPNS_K2_E : SPNS_F32_K2_E, K2_T = D ? SPNS_K2_T : SPNS_F32_K2_T;
-    static constexpr int K5_E = D ? SPNS_K5_E : SPNS_F32_K5_E, K5_T = D ? 128 : SPNS_F32_K5_T;
+    static constexpr int K5_E = D ? SPNS_K5_E : SPNS_F32_K5_E, K5_T = D ? SPNS_K5_T : SPNS_F32_K5_T;
     static constexpr int Z_E = D ? SPNS_Z_E : SPNS_F32_Z_E, Z_T = D ? SPNS_Z_THREADS : SPNS_F32_Z_T;
     static constexpr bool Z_STAGE = D ? SPNS_Z_STAGE : SPNS_F32_Z_STAGE;
     static constexpr int Z_E_ROT = D ? SPNS_Z_E_ROT : SPNS_F32_Z_E_ROT;   // rotational/velocity z pass

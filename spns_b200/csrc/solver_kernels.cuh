@@ -85,11 +85,18 @@ __device__ __forceinline__ int ffreq(int a, int M) { return a <= M / 2 ? a : a -
 #ifndef SPNS_K2_MINB
 #define SPNS_K2_MINB SPNS_AX_MINB
 #endif
+#ifndef SPNS_K1_MINB
+#define SPNS_K1_MINB SPNS_AX_MINB
+#endif
+#ifndef SPNS_K5_MINB
+#define SPNS_K5_MINB SPNS_AX_MINB
+#endif
 #ifndef SPNS_F32_AX_MINB
 #define SPNS_F32_AX_MINB 2
 #endif
 template <typename T, int PASS> struct AxisMinBlocks {
-    static constexpr int N = sizeof(T) == 8 ? ((PASS == 2 || PASS == 4) ? SPNS_K2_MINB : SPNS_AX_MINB) : SPNS_F32_AX_MINB;
+    static constexpr int N = sizeof(T) == 8 ? ((PASS == 2 || PASS == 4) ? SPNS_K2_MINB : PASS == 1 ? SPNS_K1_MINB : SPNS_K5_MINB)
+                                            : SPNS_F32_AX_MINB;
 };
 
 // Field counts of the work buffers per mode.

@@ -464,6 +464,11 @@ int spns_create(const spns_hit_args *args, const double *file_uvw, spns_handle *
         rc = file_init(h, file_uvw, uvw);
         if (!rc) rc = upload_state(h, uvw.data());
         if (rc) { g_create_error = h->err; return cleanup(rc); }
+    } else if (a.k41_ranks < 0) {
+        // zero state: the caller sets the field (no host-side K41 draw of the whole box)
+        const bool okz0 = cudaMemsetAsync(h->U, 0, s0, h->st) == cudaSuccess &&
+                          (!h->Ulo || cudaMemsetAsync(h->Ulo, 0, s0, h->st) == cudaSuccess);
+        if (!okz0) return cleanup(spns_fail(nullptr, SPNS_ERR_CUDA, "state initialisation failed"));
     } else {
         k41_host(h, uvw);
         rc = upload_state(h, uvw.data());

@@ -80,7 +80,8 @@ class GpuBackend:
 
     def create(self, req: SolveRequest, priority: int = 0):
         from .hit import HIT
-        h = HIT(req.args, precision=req.precision, device=self.device, stream_priority=priority)
+        # the state comes from the checkpoint or the seed: no host-side K41 draw at creation
+        h = HIT(req.args, precision=req.precision, device=self.device, stream_priority=priority, k41_ranks=-1)
         if req.init is not None:
             h.checkpoint_load(req.init)
         else:

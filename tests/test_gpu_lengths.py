@@ -1,7 +1,7 @@
 """GPU step against the oracle at the FFT lengths the benchmark configurations run.
 
-The forced 512^3 DNS transforms at length 768, the LES configuration and the
-served N=256 runs at 384, the served N=128 runs at 192.  Each pass kernel is a
+The forced 512^3 DNS transforms at length 768 (its 1024^3 stretch at 1536), the
+LES configuration and the served N=256 runs at 384, the served N=128 runs at 192.  Each pass kernel is a
 separate instantiation per length (values per thread, threads per pencil,
 exchange layouts, warp or block barriers), so parity at 48..96 says nothing
 about them.  Reduced anisotropic boxes put one axis at the benchmark length and
@@ -20,7 +20,7 @@ Forms, as in src/HIT_LES.cpp:9-25, 74-125, 130-192:
 
 Bar: relative L2 of the spectral state <= 1e-12 after 10 steps, dt equal to 1e-13
 at every step, as for the short lengths.  The compensated FP32 form is compared
-with the FP64 form at length 768 on every axis: E(K) within 1e-5 per shell.
+with the FP64 form at lengths 768 and 1536 on every axis: E(K) within 1e-5 per shell.
 """
 import numpy as np
 import pytest
@@ -36,6 +36,7 @@ BOXES = {
     "x768": (512, 32, 32), "y768": (32, 512, 32), "z768": (32, 32, 512),
     "x384": (256, 32, 32), "y384": (32, 256, 32), "z384": (32, 32, 256),
     "xyz192": (128, 128, 128),
+    "x1536": (1024, 32, 32), "y1536": (32, 1024, 32), "z1536": (32, 32, 1024),
 }
 FORMS = {
     "bench": (0, dict(self_adaptive=True), dict(eps_forcing=0.1)),
@@ -78,7 +79,7 @@ def test_step_parity_at_benchmark_lengths(box_name, form_name):
     gpu.close()
 
 
-@pytest.mark.parametrize("box_name", ["x768", "y768", "z768"])
+@pytest.mark.parametrize("box_name", ["x768", "y768", "z768", "x1536", "y1536", "z1536"])
 def test_fp32_form_at_length_768(box_name):
     """Compensated FP32 form against FP64, same broadband field, 20 CFL steps of the bench form."""
     from spns_b200.hit import HIT, SPNS_FP64, SPNS_FP32_HILO
