@@ -346,7 +346,21 @@ struct PrecOps {
     int (*seed_draw)(spns_handle *h, unsigned long long seed, int lim_x, int lim_y, int lim_z); // Philox field, unscaled
     int (*invariant_spectra)(spns_handle *h, double *out);    // 5 spectra of the gradient invariants
     int (*slab_phase)(spns_handle *h, int phase);             // one phase of a slab-decomposed step
+    // one step of n members of h0's class in one launch per pass (device table `tab`), on stream st
+    int (*batch_step)(spns_handle *h0, const spns::BatchMember *tab, int n, cudaStream_t st);
 };
+
+// Lengths with batched pass kernels (ensembles of small boxes).
+#define SPNS_DISPATCH_BATCH(Lval, call)                                                     \
+    switch (Lval) {                                                                          \
+    case 48: { constexpr int LL = 48; call; } break;                                         \
+    case 72: { constexpr int LL = 72; call; } break;                                         \
+    case 96: { constexpr int LL = 96; call; } break;                                         \
+    case 144: { constexpr int LL = 144; call; } break;                                       \
+    case 192: { constexpr int LL = 192; call; } break;                                       \
+    default: return spns_fail(h, SPNS_ERR_UNSUPPORTED_SIZE, "no batched kernels at FFT length %d", Lval); \
+    }
+inline bool spns_batch_length(int L) { return L == 48 || L == 72 || L == 96 || L == 144 || L == 192; }
 extern const PrecOps spns_ops_f64;
 extern const PrecOps spns_ops_f32;
 inline const PrecOps &spns_ops(const spns_handle *h) { return h->prec == SPNS_FP64 ? spns_ops_f64 : spns_ops_f32; }

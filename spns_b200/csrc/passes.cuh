@@ -556,8 +556,89 @@ template <typename T> struct Passes {
         }
     }
 
+    // ---- batched step of same-class boxes (ensembles) ----
+    // Every member of the table has h0's geometry, form, launch shapes and the
+    // Adams-Bashforth scheme without constant-power forcing or edge correction.
+    template <int L, int MODE, int ALT> static cudaError_t launch_k1b(spns_handle *h, const spns::BatchMember *tab, int n, cudaStream_t st) {
+        using S = ShapeK1A<T, L, ALT>;
+        auto kern = spns::k1_inv_x_batch<T, L, S::E, S::P, MODE>;
+        cudaError_t e = spns_set_smem(kern, S::SMEM_ROW);
+        if (e != cudaSuccess) return e;
+        kern<<<dim3((h->g.Kz + S::P - 1) / S::P, h->g.Ky, n), S::THREADS, S::SMEM_ROW, st>>>(h->g, tab, tw(h, L));
+        return cudaGetLastError();
+    }
+    template <int L, int MODE, int ALT> static cudaError_t launch_k2b(spns_handle *h, const spns::BatchMember *tab, int n, cudaStream_t st) {
+        using S = ShapeK2A<T, L, ALT>;
+        auto kern = spns::k2_inv_y_batch<T, L, S::E, S::P, MODE>;
+        cudaError_t e = spns_set_smem(kern, S::SMEM_ROW);
+        if (e != cudaSuccess) return e;
+        kern<<<dim3((h->g.Kz + S::P - 1) / S::P, h->g.Mx, n), S::THREADS, S::SMEM_ROW, st>>>(h->g, tab, tw(h, L));
+        return cudaGetLastError();
+    }
+    template <int L, int MODE, int ALT> static cudaError_t launch_k3b(spns_handle *h, const spns::BatchMember *tab, int n, cudaStream_t st) {
+        using S3 = Shape3<T, L, MODE, ALT>;
+        constexpr bool STAGE = MODE == spns::MODE_LES && sizeof(T) == 4 && SPNS_F32_Z_STAGE_LES;
+        auto kern = spns::k3_z_batch<T, L, S3::E, S3::P, MODE, STAGE>;
+        const size_t smem = S3::SMEM + (size_t)S3::P * (STAGE ? 9 : 0) * h->g.Kz * sizeof(C);
+        cudaError_t e = spns_set_smem(kern, smem);
+        if (e != cudaSuccess) return e;
+        const long long npen = (long long)h->g.Mx * h->g.My;
+        kern<<<dim3((unsigned)((npen + S3::P - 1) / S3::P), 1, n), S3::THREADS, smem, st>>>(h->g, tab, tw(h, L));
+        return cudaGetLastError();
+    }
+    template <int L, int MODE, int ALT> static cudaError_t launch_k4b(spns_handle *h, const spns::BatchMember *tab, int n, cudaStream_t st) {
+        using S = ShapeK2A<T, L, ALT>;
+        auto kern = spns::k4_fwd_y_batch<T, L, S::E, S::P, MODE>;
+        cudaError_t e = spns_set_smem(kern, S::SMEM_ROW);
+        if (e != cudaSuccess) return e;
+        kern<<<dim3((h->g.Kz + S::P - 1) / S::P, h->g.Mx, n), S::THREADS, S::SMEM_ROW, st>>>(h->g, tab, tw(h, L));
+        return cudaGetLastError();
+    }
+    template <int L, int MODE, int ALT> static cudaError_t launch_k5b(spns_handle *h, const spns::BatchMember *tab, int n, cudaStream_t st) {
+        using S = ShapeK5A<T, L, ALT>;
+        auto kern = spns::k5_fwd_x_batch<T, L, S::E, S::P, MODE>;
+        cudaError_t e = spns_set_smem(kern, S::SMEM_ROW);
+        if (e != cudaSuccess) return e;
+        kern<<<dim3((h->g.Kz + S::P - 1) / S::P, h->g.Ky, n), S::THREADS, S::SMEM_ROW, st>>>(h->g, tab, tw(h, L));
+        return cudaGetLastError();
+    }
+#define SPNS_SELECT_B(name, idx)                                                                                       \
+    template <int L, int MODE> static cudaError_t sel_##name(spns_handle *h, const spns::BatchMember *tab, int n, cudaStream_t st) { \
+        if constexpr (shape_alt_ok<L, MODE>())                                                                         \
+            if (h->shape_alt[idx]) return launch_##name<L, MODE, 1>(h, tab, n, st);                                    \
+        return launch_##name<L, MODE, 0>(h, tab, n, st);                                                               \
+    }
+    SPNS_SELECT_B(k1b, 1)
+    SPNS_SELECT_B(k2b, 2)
+    SPNS_SELECT_B(k3b, 3)
+    SPNS_SELECT_B(k4b, 4)
+    SPNS_SELECT_B(k5b, 5)
+#undef SPNS_SELECT_B
+    static int batch_step(spns_handle *h, const spns::BatchMember *tab, int n, cudaStream_t st) {
+        const int mode = h->a.isLES ? spns::MODE_LES : spns::MODE_ADV;
+        spns::k_reset_max_batch<<<n, 1, 0, st>>>(tab);
+        CKL();
+#define BATCH_PASSES(MD)                                                                  \
+        SPNS_DISPATCH_BATCH(h->g.Mx, LAUNCH((sel_k1b<LL, MD>(h, tab, n, st))));           \
+        SPNS_DISPATCH_BATCH(h->g.My, LAUNCH((sel_k2b<LL, MD>(h, tab, n, st))));           \
+        SPNS_DISPATCH_BATCH(h->g.Mz, LAUNCH((sel_k3b<LL, MD>(h, tab, n, st))));           \
+        SPNS_DISPATCH_BATCH(h->g.My, LAUNCH((sel_k4b<LL, MD>(h, tab, n, st))));           \
+        SPNS_DISPATCH_BATCH(h->g.Mx, LAUNCH((sel_k5b<LL, MD>(h, tab, n, st))));
+        if (mode == spns::MODE_LES) { BATCH_PASSES(spns::MODE_LES) }
+        else { BATCH_PASSES(spns::MODE_ADV) }
+#undef BATCH_PASSES
+        {
+            const int nk = h->g.Kx * h->g.Kz;
+            spns::k6_sweep_batch<T><<<dim3((nk + 255) / 256, h->g.Ky, n), 256, 0, st>>>(h->g, tab);
+            CKL();
+        }
+        spns::k_finish_step_batch<<<n, 1, 0, st>>>(tab);
+        CKL();
+        return SPNS_OK;
+    }
+
     static constexpr PrecOps ops() {
         return PrecOps{&step_once, &run_velocity, &shell_sums, &forcing_scale, &conj_correction, &seed_draw, &invariant_spectra,
-                       &slab_phase};
+                       &slab_phase, &batch_step};
     }
 };

@@ -113,9 +113,8 @@ template <int MODE> struct Fields {
 //   w_z=i(kx v-ky u) (ky is the block's, kx the row's)   ADV/LES: u,v,w, du/dx, dv/dx, dw/dx
 // ===========================================================================
 template <typename T, int L, int E, int P, int MODE>
-__global__ void __launch_bounds__(P *(L / E), AxisMinBlocks<T, 1>::N) k1_inv_x(Geo g, const cx<T> *__restrict__ u, const cx<T> *__restrict__ v,
-                                                       const cx<T> *__restrict__ w, cx<T> *__restrict__ out,
-                                                       const cx<T> *__restrict__ tw) {
+__device__ __forceinline__ void k1_inv_x_body(Geo g, const cx<T> *__restrict__ u, const cx<T> *__restrict__ v,
+                                              const cx<T> *__restrict__ w, cx<T> *__restrict__ out, const cx<T> *__restrict__ tw) {
     extern __shared__ __align__(16) unsigned char smraw[];
     const int tid = threadIdx.x, p = tid % P, q = tid / P;
     const int iy = blockIdx.y, kz = blockIdx.x * P + p;
@@ -164,8 +163,8 @@ __global__ void __launch_bounds__(P *(L / E), AxisMinBlocks<T, 1>::N) k1_inv_x(G
 //   ADV/LES: u,v,w, du/dx,dv/dx,dw/dx, du/dy,dv/dy,dw/dy
 // ===========================================================================
 template <typename T, int L, int E, int P, int MODE>
-__global__ void __launch_bounds__(P *(L / E), AxisMinBlocks<T, 2>::N) k2_inv_y(Geo g, const cx<T> *__restrict__ in, cx<T> *__restrict__ out,
-                                                       const cx<T> *__restrict__ tw) {
+__device__ __forceinline__ void k2_inv_y_body(Geo g, const cx<T> *__restrict__ in, cx<T> *__restrict__ out,
+                                              const cx<T> *__restrict__ tw) {
     extern __shared__ __align__(16) unsigned char smraw[];
     const int tid = threadIdx.x, p = tid % P, q = tid / P;
     const int x = blockIdx.y, kz = blockIdx.x * P + p;
@@ -457,9 +456,9 @@ template <typename T, int MODE, int THREADS> struct K3MinBlocks {
     static constexpr int B = REGS > 0 ? 65536 / (REGS * THREADS) : 1;
     static constexpr int N = B < 1 ? 1 : B;
 };
-template <typename T, int L, int E, int P, int MODE, bool STAGE = false>
-__global__ void __launch_bounds__(P *(L / E), K3MinBlocks<T, MODE, P *(L / E)>::N) k3_z(Geo g, cx<T> *__restrict__ buf, StepConsts c, DevScalars *ds,
-                                                   double *__restrict__ phys, const cx<T> *__restrict__ tw) {
+template <typename T, int L, int E, int P, int MODE, bool STAGE>
+__device__ __forceinline__ void k3_z_body(Geo g, cx<T> *__restrict__ buf, const StepConsts &c, DevScalars *ds,
+                                          double *__restrict__ phys, const cx<T> *__restrict__ tw) {
     extern __shared__ __align__(16) unsigned char smraw[];
     constexpr int Q = L / E;
     const int tid = threadIdx.x, p = tid / Q, q = tid % Q;
@@ -893,8 +892,8 @@ template <int MODE> __host__ __device__ constexpr int k4_in_field(int f) { retur
 // LES: G_i += i ky t_i2 (SGS divergence, y part).
 // ===========================================================================
 template <typename T, int L, int E, int P, int MODE>
-__global__ void __launch_bounds__(P *(L / E), AxisMinBlocks<T, 4>::N) k4_fwd_y(Geo g, const cx<T> *__restrict__ in, cx<T> *__restrict__ out,
-                                                       const cx<T> *__restrict__ tw) {
+__device__ __forceinline__ void k4_fwd_y_body(Geo g, const cx<T> *__restrict__ in, cx<T> *__restrict__ out,
+                                              const cx<T> *__restrict__ tw) {
     extern __shared__ __align__(16) unsigned char smraw[];
     const int tid = threadIdx.x, p = tid % P, q = tid / P;
     const int x = blockIdx.y, kz = blockIdx.x * P + p;
@@ -953,8 +952,8 @@ __global__ void __launch_bounds__(P *(L / E), AxisMinBlocks<T, 4>::N) k4_fwd_y(G
 // (S0).  Block = (kz chunk, iy).  LES: G_i += i kx t_i1 (SGS divergence, x part).
 // ===========================================================================
 template <typename T, int L, int E, int P, int MODE>
-__global__ void __launch_bounds__(P *(L / E), AxisMinBlocks<T, 5>::N) k5_fwd_x(Geo g, const cx<T> *__restrict__ in, cx<T> *__restrict__ G,
-                                                          const cx<T> *__restrict__ tw) {
+__device__ __forceinline__ void k5_fwd_x_body(Geo g, const cx<T> *__restrict__ in, cx<T> *__restrict__ G,
+                                              const cx<T> *__restrict__ tw) {
     extern __shared__ __align__(16) unsigned char smraw[];
     const int tid = threadIdx.x, p = tid % P, q = tid / P;
     const int iy = blockIdx.y, kz = blockIdx.x * P + p;
@@ -1007,9 +1006,9 @@ __global__ void __launch_bounds__(P *(L / E), AxisMinBlocks<T, 5>::N) k5_fwd_x(G
 // are unused (null).
 // ===========================================================================
 template <typename T, bool SELF>
-__global__ void __launch_bounds__(256) k6_sweep(Geo g, const cx<T> *__restrict__ G, const cx<T> *U, const cx<T> *Ulo, cx<T> *R,
-                                                cx<T> *Uout, cx<T> *Uoutlo, const cx<T> *Un1, const cx<T> *Un1lo, StepConsts c,
-                                                const DevScalars *__restrict__ ds) {
+__device__ __forceinline__ void k6_sweep_body(Geo g, const cx<T> *__restrict__ G, const cx<T> *U, const cx<T> *Ulo, cx<T> *R,
+                                              cx<T> *Uout, cx<T> *Uoutlo, const cx<T> *Un1, const cx<T> *Un1lo, const StepConsts &c,
+                                              const DevScalars *__restrict__ ds) {
     constexpr bool HILO = sizeof(T) == 4;
     const int iy = blockIdx.y;
     const int n = g.Kx * g.Kz;
@@ -1517,6 +1516,104 @@ static __global__ void k_dft_axis(const double2 *__restrict__ in, double2 *__res
         }
         out[ob + (long long)kk * es_out] = make_double2(sr, si);
     }
+}
+
+// ===========================================================================
+// Kernels of the passes, for one box and for a batch of boxes of the same
+// geometry and launch shape.  A batch runs one launch per pass for all its
+// members: blockIdx.z selects the member, whose buffers, scalars and constants
+// come from a device table (BatchMember).  The arithmetic is the one-box kernel's.
+// ===========================================================================
+template <typename T, int L, int E, int P, int MODE>
+__global__ void __launch_bounds__(P *(L / E), AxisMinBlocks<T, 1>::N) k1_inv_x(Geo g, const cx<T> *__restrict__ u, const cx<T> *__restrict__ v,
+                                                                           const cx<T> *__restrict__ w, cx<T> *__restrict__ out,
+                                                                           const cx<T> *__restrict__ tw) {
+    k1_inv_x_body<T, L, E, P, MODE>(g, u, v, w, out, tw);
+}
+template <typename T, int L, int E, int P, int MODE>
+__global__ void __launch_bounds__(P *(L / E), AxisMinBlocks<T, 2>::N) k2_inv_y(Geo g, const cx<T> *__restrict__ in, cx<T> *__restrict__ out,
+                                                                           const cx<T> *__restrict__ tw) {
+    k2_inv_y_body<T, L, E, P, MODE>(g, in, out, tw);
+}
+template <typename T, int L, int E, int P, int MODE, bool STAGE = false>
+__global__ void __launch_bounds__(P *(L / E), K3MinBlocks<T, MODE, P *(L / E)>::N) k3_z(Geo g, cx<T> *__restrict__ buf, StepConsts c,
+                                                                                        DevScalars *ds, double *__restrict__ phys,
+                                                                                        const cx<T> *__restrict__ tw) {
+    k3_z_body<T, L, E, P, MODE, STAGE>(g, buf, c, ds, phys, tw);
+}
+template <typename T, int L, int E, int P, int MODE>
+__global__ void __launch_bounds__(P *(L / E), AxisMinBlocks<T, 4>::N) k4_fwd_y(Geo g, const cx<T> *__restrict__ in, cx<T> *__restrict__ out,
+                                                                           const cx<T> *__restrict__ tw) {
+    k4_fwd_y_body<T, L, E, P, MODE>(g, in, out, tw);
+}
+template <typename T, int L, int E, int P, int MODE>
+__global__ void __launch_bounds__(P *(L / E), AxisMinBlocks<T, 5>::N) k5_fwd_x(Geo g, const cx<T> *__restrict__ in, cx<T> *__restrict__ G,
+                                                                           const cx<T> *__restrict__ tw) {
+    k5_fwd_x_body<T, L, E, P, MODE>(g, in, G, tw);
+}
+template <typename T, bool SELF>
+__global__ void __launch_bounds__(256) k6_sweep(Geo g, const cx<T> *__restrict__ G, const cx<T> *U, const cx<T> *Ulo, cx<T> *R, cx<T> *Uout,
+                                                cx<T> *Uoutlo, const cx<T> *Un1, const cx<T> *Un1lo, StepConsts c,
+                                                const DevScalars *__restrict__ ds) {
+    k6_sweep_body<T, SELF>(g, G, U, Ulo, R, Uout, Uoutlo, Un1, Un1lo, c, ds);
+}
+
+// One member of a batched launch.  The state is [3][S0] (hi parts; Ulo the
+// compensated form's lo parts, else null), R the previous right-hand side, B1/B2
+// the S1/S2 work buffers (B2 also holds the nonlinear term after the x pass).
+struct BatchMember {
+    void *U, *Ulo, *R, *B1, *B2;
+    DevScalars *ds;
+    StepConsts c;
+};
+template <typename T, int L, int E, int P, int MODE>
+__global__ void __launch_bounds__(P *(L / E), AxisMinBlocks<T, 1>::N) k1_inv_x_batch(Geo g, const BatchMember *__restrict__ tab,
+                                                                                 const cx<T> *__restrict__ tw) {
+    const BatchMember &m = tab[blockIdx.z];
+    const cx<T> *U = static_cast<const cx<T> *>(m.U);
+    k1_inv_x_body<T, L, E, P, MODE>(g, U, U + g.S0, U + 2 * g.S0, static_cast<cx<T> *>(m.B1), tw);
+}
+template <typename T, int L, int E, int P, int MODE>
+__global__ void __launch_bounds__(P *(L / E), AxisMinBlocks<T, 2>::N) k2_inv_y_batch(Geo g, const BatchMember *__restrict__ tab,
+                                                                                 const cx<T> *__restrict__ tw) {
+    const BatchMember &m = tab[blockIdx.z];
+    k2_inv_y_body<T, L, E, P, MODE>(g, static_cast<const cx<T> *>(m.B1), static_cast<cx<T> *>(m.B2), tw);
+}
+template <typename T, int L, int E, int P, int MODE, bool STAGE = false>
+__global__ void __launch_bounds__(P *(L / E), K3MinBlocks<T, MODE, P *(L / E)>::N) k3_z_batch(Geo g, const BatchMember *__restrict__ tab,
+                                                                                              const cx<T> *__restrict__ tw) {
+    const BatchMember &m = tab[blockIdx.z];
+    k3_z_body<T, L, E, P, MODE, STAGE>(g, static_cast<cx<T> *>(m.B2), m.c, m.ds, nullptr, tw);
+}
+template <typename T, int L, int E, int P, int MODE>
+__global__ void __launch_bounds__(P *(L / E), AxisMinBlocks<T, 4>::N) k4_fwd_y_batch(Geo g, const BatchMember *__restrict__ tab,
+                                                                                 const cx<T> *__restrict__ tw) {
+    const BatchMember &m = tab[blockIdx.z];
+    k4_fwd_y_body<T, L, E, P, MODE>(g, static_cast<const cx<T> *>(m.B2), static_cast<cx<T> *>(m.B1), tw);
+}
+template <typename T, int L, int E, int P, int MODE>
+__global__ void __launch_bounds__(P *(L / E), AxisMinBlocks<T, 5>::N) k5_fwd_x_batch(Geo g, const BatchMember *__restrict__ tab,
+                                                                                 const cx<T> *__restrict__ tw) {
+    const BatchMember &m = tab[blockIdx.z];
+    k5_fwd_x_body<T, L, E, P, MODE>(g, static_cast<const cx<T> *>(m.B1), static_cast<cx<T> *>(m.B2), tw);
+}
+// Adams-Bashforth members only (the kappa scheme swaps state buffers every step).
+template <typename T>
+__global__ void __launch_bounds__(256) k6_sweep_batch(Geo g, const BatchMember *__restrict__ tab) {
+    const BatchMember &m = tab[blockIdx.z];
+    cx<T> *U = static_cast<cx<T> *>(m.U), *Ulo = static_cast<cx<T> *>(m.Ulo);
+    k6_sweep_body<T, false>(g, static_cast<const cx<T> *>(m.B2), U, Ulo, static_cast<cx<T> *>(m.R), U, Ulo, nullptr, nullptr, m.c, m.ds);
+}
+static __global__ void k_reset_max_batch(const BatchMember *__restrict__ tab) {
+    DevScalars *ds = tab[blockIdx.x].ds;
+    for (int i = 0; i < 4; i++) ds->max_bits[i] = 0ull;
+    ds->sumsq_phys = 0.0;
+}
+static __global__ void k_finish_step_batch(const BatchMember *__restrict__ tab) {
+    const BatchMember &m = tab[blockIdx.x];
+    recalc_dt(m.c, m.ds);
+    m.ds->time = m.ds->time + m.ds->dt;
+    m.ds->iter += 1;
 }
 
 } // namespace spns

@@ -1194,6 +1194,13 @@ extern "C" int spns_slab_buffers(spns_handle *h, void **send, void **recv, size_
 // are kept per pattern of state-buffer parities (the kappa scheme swaps its
 // buffers every step; the graph bakes the pointers in).
 // ---------------------------------------------------------------------------
+// Members of the same class (precision, box, form, launch shapes; Adams-Bashforth
+// without constant-power forcing or edge correction) step in one launch per pass
+// (Passes::batch_step) over a device table of their buffers and constants.
+struct EnsembleClass {
+    std::vector<int> idx;
+    BatchMember *tab = nullptr;
+};
 struct spns_ensemble {
     std::vector<spns_handle *> m;
     cudaStream_t st = nullptr;
@@ -1202,7 +1209,49 @@ struct spns_ensemble {
     std::map<std::vector<bool>, cudaGraphExec_t> graphs;
     std::string err;
     int device = 0;
+    bool grouped = false;
+    std::vector<EnsembleClass> classes;             // batched classes (two members or more)
+    std::vector<int> single;                        // members stepped on their own branch
 };
+
+static bool batchable(const spns_handle *h) {
+    return h->slab_ranks == 0 && !h->a.isSelfAdaptive && !(h->a.eps_forcing > 0.0) && (h->a.isLES || h->a.nonlinear_form == 2) &&
+           spns_batch_length(h->g.Mx) && spns_batch_length(h->g.My) && spns_batch_length(h->g.Mz);
+}
+
+// Classes of members that can share launches; the tables are filled once (their
+// buffers do not move under the Adams-Bashforth scheme).
+static int ensemble_group(spns_ensemble *e) {
+    std::map<std::vector<long long>, std::vector<int>> by;
+    for (int i = 0; i < (int)e->m.size(); i++) {
+        const spns_handle *h = e->m[i];
+        if (!batchable(h)) { e->single.push_back(i); continue; }
+        const Geo &g = h->g;
+        std::vector<long long> key = {h->prec, g.Kx, g.Ky, g.Kz, g.Mx, g.My, g.Mz, g.sx, g.sy, g.sz, h->a.isLES};
+        for (int k = 1; k <= 5; k++) key.push_back(h->shape_alt[k]);
+        by[key].push_back(i);
+    }
+    for (auto &kv : by) {
+        if (kv.second.size() < 2) { e->single.push_back(kv.second[0]); continue; }
+        EnsembleClass c;
+        c.idx = kv.second;
+        std::vector<BatchMember> host(c.idx.size());
+        for (size_t j = 0; j < c.idx.size(); j++) {
+            const spns_handle *h = e->m[c.idx[j]];
+            host[j].U = h->U; host[j].Ulo = h->Ulo; host[j].R = h->R; host[j].B1 = h->B1; host[j].B2 = h->B2;
+            host[j].ds = h->ds; host[j].c = h->c;
+        }
+        if (cudaMalloc(&c.tab, sizeof(BatchMember) * host.size()) != cudaSuccess ||
+            cudaMemcpy(c.tab, host.data(), sizeof(BatchMember) * host.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+            if (c.tab) cudaFree(c.tab);
+            e->err = "ensemble table allocation failed";
+            return SPNS_ERR_OUT_OF_MEMORY;
+        }
+        e->classes.push_back(c);
+    }
+    e->grouped = true;
+    return SPNS_OK;
+}
 
 static std::vector<bool> ensemble_parity(const spns_ensemble *e) {
     std::vector<bool> p(e->m.size());
@@ -1212,6 +1261,7 @@ static std::vector<bool> ensemble_parity(const spns_ensemble *e) {
 
 static void ensemble_free(spns_ensemble *e) {
     if (!e) return;
+    for (auto &c : e->classes) if (c.tab) cudaFree(c.tab);
     for (auto &kv : e->graphs) cudaGraphExecDestroy(kv.second);
     for (auto ev : e->join) if (ev) cudaEventDestroy(ev);
     if (e->fork) cudaEventDestroy(e->fork);
@@ -1290,6 +1340,10 @@ extern "C" int spns_ensemble_step(spns_ensemble *e, int nsteps) {
             }
             continue;
         }
+        if (!e->grouped) {
+            const int rg = ensemble_group(e);
+            if (rg) return rg;
+        }
         const std::vector<bool> par = ensemble_parity(e);
         auto it = e->graphs.find(par);
         if (it == e->graphs.end()) {
@@ -1299,7 +1353,20 @@ extern "C" int spns_ensemble_step(spns_ensemble *e, int nsteps) {
             ECK(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
             int r = SPNS_OK;
             cudaError_t ce = cudaEventRecord(e->fork, e->st);
-            for (int i = 0; i < n && r == SPNS_OK && ce == cudaSuccess; i++) {
+            // one branch per batched class (one launch per pass for all its members) ...
+            for (size_t k = 0; k < e->classes.size() && r == SPNS_OK && ce == cudaSuccess; k++) {
+                const EnsembleClass &c = e->classes[k];
+                spns_handle *h = e->m[c.idx[0]];
+                ce = cudaStreamWaitEvent(h->st, e->fork, 0);
+                if (ce != cudaSuccess) break;
+                r = spns_ops(h).batch_step(h, c.tab, (int)c.idx.size(), h->st);
+                if (r) { e->err = "batched class of member " + std::to_string(c.idx[0]) + ": " + h->err; break; }
+                ce = cudaEventRecord(e->join[c.idx[0]], h->st);
+                if (ce == cudaSuccess) ce = cudaStreamWaitEvent(e->st, e->join[c.idx[0]], 0);
+            }
+            // ... and one per other member
+            for (size_t k = 0; k < e->single.size() && r == SPNS_OK && ce == cudaSuccess; k++) {
+                const int i = e->single[k];
                 spns_handle *h = e->m[i];
                 ce = cudaStreamWaitEvent(h->st, e->fork, 0);
                 if (ce != cudaSuccess) break;

@@ -157,3 +157,30 @@ def test_estimate_matches_the_allocation():
         # allocation granularity (2 MiB pages) and the stream's own memory
         assert est <= used + (64 << 20) and used <= est + (64 << 20), (est, used)
         h.close()
+
+
+def test_ensemble_batched_classes_equal_their_runs_alone():
+    """Members of one class (same precision, box, form and launch shapes; Adams-Bashforth)
+    step in one launch per pass for the whole class; each still reaches bit for bit the
+    state it reaches alone.  Mixed with members that keep their own branch."""
+    from spns_b200.hit import HIT, Ensemble
+    specs = [(32, dict(les=0.10), 1, 2), (32, dict(les=0.15), 1, 2), (32, dict(les=0.20, rotating=(0.0, 0.0, 1.0)), 1, 2),
+             (48, dict(), 0, 2), (48, dict(), 0, 2), (32, dict(les=0.17), 0, 2), (32, dict(les=0.12), 0, 2),
+             (32, dict(self_adaptive=True), 0, 0), (48, dict(les=0.1), 1, 2)]
+
+    def make(i, N, opts, prec, form):
+        h = HIT(make_args(N, nu=2e-3, **opts), precision=prec, nonlinear_form=form, k41_ranks=-1)
+        h.seed_field(100 + i, 3.0)
+        return h
+
+    members = [make(i, *sp) for i, sp in enumerate(specs)]
+    alone = [make(i, *sp) for i, sp in enumerate(specs)]
+    for h in alone:
+        h.New_Fractional_Step_Method(9)
+    ens = Ensemble(members)
+    ens.step(2)
+    ens.step(7)
+    for h, ref in zip(members, alone):
+        assert np.array_equal(h.get_compact(), ref.get_compact())
+        assert h.gettime() == ref.gettime() and h.getAt() == ref.getAt()
+    ens.close()
