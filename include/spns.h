@@ -247,6 +247,15 @@ int spns_ensemble_create(spns_handle *const *members, int n, spns_ensemble **out
 int spns_ensemble_step(spns_ensemble *e, int nsteps);
 int spns_ensemble_destroy(spns_ensemble *e);
 const char *spns_ensemble_last_error(spns_ensemble *e);
+/* Batched classes (off by default): members of one class -- same precision, box,
+ * form (advective or LES) and launch shapes, Adams-Bashforth, no constant-power
+ * forcing -- step in one launch per pass for the whole class (blockIdx.z selects
+ * the member from a device table of its buffers and constants) instead of one
+ * graph branch each.  Results are bit for bit those of the branches.  Measured on
+ * a B200 with FP32 LES boxes: 64 boxes of 32^3 73.0k against 72.4k box-steps/s,
+ * 64 of 48^3 29.4k against 30.2k, the 64-box mix of 32..96^3 7.9k against 8.4k:
+ * the boxes' own kernels bound an ensemble, not launches. */
+int spns_ensemble_set_batched(spns_ensemble *e, int on);
 
 /* Per-kernel CUDA-event profile of the next max_steps calls of one step
  * (events recorded on the handle's stream between the kernels of a step). */

@@ -1209,6 +1209,7 @@ struct spns_ensemble {
     std::map<std::vector<bool>, cudaGraphExec_t> graphs;
     std::string err;
     int device = 0;
+    bool batched = false;                           // spns_ensemble_set_batched
     bool grouped = false;
     std::vector<EnsembleClass> classes;             // batched classes (two members or more)
     std::vector<int> single;                        // members stepped on their own branch
@@ -1225,7 +1226,7 @@ static int ensemble_group(spns_ensemble *e) {
     std::map<std::vector<long long>, std::vector<int>> by;
     for (int i = 0; i < (int)e->m.size(); i++) {
         const spns_handle *h = e->m[i];
-        if (!batchable(h)) { e->single.push_back(i); continue; }
+        if (!e->batched || !batchable(h)) { e->single.push_back(i); continue; }
         const Geo &g = h->g;
         std::vector<long long> key = {h->prec, g.Kx, g.Ky, g.Kz, g.Mx, g.My, g.Mz, g.sx, g.sy, g.sz, h->a.isLES};
         for (int k = 1; k <= 5; k++) key.push_back(h->shape_alt[k]);
@@ -1311,6 +1312,21 @@ extern "C" int spns_ensemble_destroy(spns_ensemble *e) {
 }
 
 extern "C" const char *spns_ensemble_last_error(spns_ensemble *e) { return e ? e->err.c_str() : ""; }
+
+extern "C" int spns_ensemble_set_batched(spns_ensemble *e, int on) {
+    if (!e) return SPNS_ERR_INVALID_ARGUMENT;
+    if (e->batched == (on != 0)) return SPNS_OK;
+    cudaSetDevice(e->device);
+    cudaStreamSynchronize(e->st);
+    for (auto &kv : e->graphs) cudaGraphExecDestroy(kv.second);
+    e->graphs.clear();
+    for (auto &c : e->classes) if (c.tab) cudaFree(c.tab);
+    e->classes.clear();
+    e->single.clear();
+    e->grouped = false;
+    e->batched = on != 0;
+    return SPNS_OK;
+}
 
 // Advances every member by nsteps steps.  Members that have not yet run a step
 // run their first one uncaptured (each on its own stream, concurrently); the

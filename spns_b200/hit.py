@@ -35,7 +35,7 @@ EXPORTED_SYMBOLS = (
     "spns_ensemble_create", "spns_ensemble_step", "spns_ensemble_destroy", "spns_ensemble_last_error",
     "spns_invariant_spectra", "spns_eddy_viscosity_stats", "spns_autotune", "spns_autotune_forget", "spns_set_shapes",
     "spns_slab_block", "spns_slab_create", "spns_slab_layout", "spns_slab_phase", "spns_slab_exchange", "spns_slab_counts",
-    "spns_slab_buffers",
+    "spns_slab_buffers", "spns_ensemble_set_batched",
 )
 
 
@@ -138,6 +138,7 @@ def lib():
         L.spns_ensemble_destroy.argtypes = [vp]
         L.spns_ensemble_last_error.argtypes = [vp]
         L.spns_ensemble_last_error.restype = C.c_char_p
+        L.spns_ensemble_set_batched.argtypes = [vp, i]
         L.spns_invariant_spectra.argtypes = [vp, dp]
         L.spns_eddy_viscosity_stats.argtypes = [vp, dp]
         L.spns_autotune.argtypes = [vp, i, ip]
@@ -433,7 +434,7 @@ class HIT:
 class Ensemble:
     """Members advanced together, one CUDA graph per step (spns_ensemble_*)."""
 
-    def __init__(self, members):
+    def __init__(self, members, batched: bool = False):
         L = lib()
         self.members = list(members)
         arr = (C.c_void_p * len(self.members))(*[m._h for m in self.members])
@@ -442,6 +443,8 @@ class Ensemble:
         if st != 0:
             raise SpnsError(st, L.spns_last_error(None).decode())
         self._e, self._L = e, L
+        if batched:
+            L.spns_ensemble_set_batched(e, 1)
 
     def step(self, nsteps: int = 1):
         st = self._L.spns_ensemble_step(self._e, int(nsteps))

@@ -168,16 +168,21 @@ def test_ensemble_batched_classes_equal_their_runs_alone():
              (48, dict(), 0, 2), (48, dict(), 0, 2), (32, dict(les=0.17), 0, 2), (32, dict(les=0.12), 0, 2),
              (32, dict(self_adaptive=True), 0, 0), (48, dict(les=0.1), 1, 2)]
 
-    def make(i, N, opts, prec, form):
-        h = HIT(make_args(N, nu=2e-3, **opts), precision=prec, nonlinear_form=form, k41_ranks=-1)
-        h.seed_field(100 + i, 3.0)
-        return h
+    def make(N, opts, prec, form):
+        return HIT(make_args(N, nu=2e-3, **opts), precision=prec, nonlinear_form=form, k41_ranks=-1)
 
-    members = [make(i, *sp) for i, sp in enumerate(specs)]
-    alone = [make(i, *sp) for i, sp in enumerate(specs)]
+    members, alone = [], []
+    for i, sp in enumerate(specs):
+        h = make(*sp)
+        h.seed_field(100 + i, 3.0)
+        blob = h.checkpoint_save()        # the same initial state, bit for bit, for the run alone
+        members.append(h)
+        a = make(*sp)
+        a.checkpoint_load(blob)
+        alone.append(a)
     for h in alone:
         h.New_Fractional_Step_Method(9)
-    ens = Ensemble(members)
+    ens = Ensemble(members, batched=True)
     ens.step(2)
     ens.step(7)
     for h, ref in zip(members, alone):
