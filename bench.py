@@ -35,6 +35,11 @@ EPS = 0.1
 C_AT = 0.5
 SEED = 2024
 METRIC = "time steps/s, forced DNS N=512 (FFT 768^3), FP64"
+# kernels behind the per-pass event names at N=512, FP64 (the z pass at length 768 is the
+# persistent pair-staged kernel)
+KERNEL_SYMBOL = {"k3_z": "k3_rot_staged<double,768,E=12,2 pencils>", "k1_inv_x": "k1_inv_x<double,768,12,4>",
+                 "k2_inv_y": "k2_inv_y<double,768,24,8>", "k4_fwd_y": "k4_fwd_y<double,768,24,8>",
+                 "k5_fwd_x": "k5_fwd_x<double,768,24,4>", "k6_sweep": "k6_sweep<double,kappa>"}
 
 
 def nu_for(N: int, eps: float = EPS) -> float:
@@ -614,7 +619,8 @@ def run_gpu(args):
         "graphs": "timed steps replay one CUDA graph per step",
         "step_algorithmic_bytes": step_bytes,
         "step_achieved_GBps": step_bytes / (ms_max / args.steps / 1e3) / 1e9,
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "roofline": {"bound": "hbm", "kernel": dom, "kernel_symbol": KERNEL_SYMBOL.get(dom, dom),
+                     "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                      "algorithmic_bytes": bytes_per[dom]},
     }

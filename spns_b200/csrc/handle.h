@@ -205,7 +205,7 @@ template <typename T, int L, int MODE, int ALT = 0> struct Shape3 {
     static constexpr int Q = L / E;
     static constexpr int ZT = ShapeSel<T>::Z_T / Q;
     static constexpr int P0 = ZT >= 32 ? 32 : ZT >= 16 ? 16 : ZT >= 8 ? 8 : ZT >= 4 ? 4 : ZT >= 2 ? 2 : 1;
-    static constexpr size_t PER_PEN = (size_t)spns::SmPencil<T, L, E>::PITCH * sizeof(spns::cx<T>) + (size_t)spns::K3Reg<T, MODE, E>::NSM * L * sizeof(T);
+    static constexpr size_t PER_PEN = (size_t)spns::pencil_pitch<T, L, E>() * sizeof(spns::cx<T>) + (size_t)spns::K3Reg<T, MODE, E>::NSM * L * sizeof(T);
     static constexpr int PMAX = (int)((200 * 1024) / PER_PEN);
     static constexpr int P = P0 <= PMAX ? P0 : PMAX >= 16 ? 16 : PMAX >= 8 ? 8 : PMAX >= 4 ? 4 : PMAX >= 2 ? 2 : 1;
     static constexpr int THREADS = P * Q;

@@ -164,7 +164,10 @@ template <typename T> struct Passes {
         constexpr bool STAGE_LES = MODE == spns::MODE_LES && sizeof(T) == 4 && SPNS_F32_Z_STAGE_LES;
         constexpr bool STAGE = STAGE_ROT || STAGE_LES;
         auto kern = spns::k3_z<T, L, S3::E, S3::P, MODE, STAGE>;
-        const size_t stage_fields = STAGE_ROT ? 2 * spns::K3StagePairs<T>::N : STAGE_LES ? 9 : 0;
+        constexpr size_t stage_fields = STAGE_ROT ? 2 * spns::K3StagePairs<T>::N : STAGE_LES ? 9 : 0;
+        // the staging is sized by Kz at run time: at most L/2+1 values per field and pencil
+        static_assert(S3::SMEM + (size_t)S3::P * stage_fields * (L / 2 + 1) * sizeof(C) <= 227 * 1024,
+                      "z-pass shared memory (exchange, physical slots and staging) exceeds 227 KB for this shape");
         const size_t smem = S3::SMEM + (size_t)S3::P * stage_fields * h->g.Kz * sizeof(C);
         cudaError_t e = spns_set_smem(kern, smem);
         if (e != cudaSuccess) return e;

@@ -25,7 +25,7 @@
 // divergence is folded into the forward passes (i kz t_i3 in K3, i ky t_i2 in
 // K4, i kx t_i1 in K5).
 #pragma once
-#include "fft_core.cuh"
+#include "fft768.cuh"
 
 namespace spns {
 
@@ -304,7 +304,7 @@ template <typename T, int L, int E>
 __device__ __forceinline__ void k3_store_pair(cx<T> (&r)[E], SmPencil<T, L, E> sm, int q, int Kz, cx<T> *A, cx<T> *B,
                                               bool fold_dz_b_into_a, T sz, bool ok, const cx<T> *__restrict__ tw) {
     constexpr int Q = L / E;
-    fft<T, L, E, false, SmPencil<T, L, E>, (32 % (L / E) == 0)>(r, sm, q, tw);
+    pencil_fft<T, L, E, false, (32 % (L / E) == 0)>(r, sm, q, tw);
 #pragma unroll
     for (int e = 0; e < E; e++) sm.at(out_row<L, E, false>(q, e)) = r[e];
     __syncthreads();
@@ -326,7 +326,7 @@ __device__ __forceinline__ void k3_store_pair(cx<T> (&r)[E], SmPencil<T, L, E> s
 template <typename T, int L, int E>
 __device__ __forceinline__ void k3_store_single(cx<T> (&r)[E], SmPencil<T, L, E> sm, int q, int Kz, cx<T> *A, bool ok,
                                                 const cx<T> *__restrict__ tw) {
-    fft<T, L, E, false, SmPencil<T, L, E>, (32 % (L / E) == 0)>(r, sm, q, tw);
+    pencil_fft<T, L, E, false, (32 % (L / E) == 0)>(r, sm, q, tw);
     if (ok) {
 #pragma unroll
         for (int e = 0; e < E; e++) {
@@ -342,7 +342,7 @@ template <typename T, int L, int E>
 __device__ __forceinline__ void k3_store_job(cx<T> (&r)[E], SmPencil<T, L, E> sm, int q, int Kz, cx<T> *A, cx<T> *B, bool fold,
                                              bool single, T sz, bool ok, const cx<T> *__restrict__ tw) {
     constexpr int Q = L / E;
-    fft<T, L, E, false, SmPencil<T, L, E>, (32 % (L / E) == 0)>(r, sm, q, tw);
+    pencil_fft<T, L, E, false, (32 % (L / E) == 0)>(r, sm, q, tw);
     if (single) {
         if (ok) {
 #pragma unroll
@@ -467,9 +467,10 @@ __device__ __forceinline__ void k3_z_body(Geo g, cx<T> *__restrict__ buf, const 
     const bool ok = pen < npen;
     const long long base = (ok ? pen : 0) * g.Kz;
     cx<T> *smc = reinterpret_cast<cx<T> *>(smraw);
-    SmPencil<T, L, E> sm{smc + p * SmPencil<T, L, E>::PITCH};
+    constexpr int PITCH = pencil_pitch<T, L, E>();
+    SmPencil<T, L, E> sm{smc + p * PITCH};
     constexpr int NREG = K3Reg<T, MODE, E>::N;
-    T *ph = reinterpret_cast<T *>(smc + P * SmPencil<T, L, E>::PITCH) + (long long)p * K3Reg<T, MODE, E>::NSM * L;
+    T *ph = reinterpret_cast<T *>(smc + P * PITCH) + (long long)p * K3Reg<T, MODE, E>::NSM * L;
     const T sz = T(g.sz);
     cx<T> *const B0 = buf + base;
 #define F(i) (B0 + (long long)(i) * g.S2)
@@ -478,9 +479,9 @@ __device__ __forceinline__ void k3_z_body(Geo g, cx<T> *__restrict__ buf, const 
     if constexpr (MODE == MODE_VEL) {
         cx<T> A[E], B[E];
         k3_load_pair<T, L, E>(A, F(0), false, F(1), false, g.Kz, sz, q, ok);
-        fft<T, L, E, true, SmPencil<T, L, E>, (32 % (L / E) == 0)>(A, sm, q, tw);
+        pencil_fft<T, L, E, true, (32 % (L / E) == 0)>(A, sm, q, tw);
         k3_load_pair<T, L, E>(B, F(2), false, nullptr, false, g.Kz, sz, q, ok);
-        fft<T, L, E, true, SmPencil<T, L, E>, (32 % (L / E) == 0)>(B, sm, q, tw);
+        pencil_fft<T, L, E, true, (32 % (L / E) == 0)>(B, sm, q, tw);
         double ss = 0.0;
 #pragma unroll
         for (int e = 0; e < E; e++) {
@@ -511,7 +512,7 @@ __device__ __forceinline__ void k3_z_body(Geo g, cx<T> *__restrict__ buf, const 
         cx<T> A[E];
         const cx<T> *src[6] = {F(0), F(1), F(2), F(3), F(4), F(5)};
         if constexpr (STAGE) {
-            cx<T> *st = smc + P * SmPencil<T, L, E>::PITCH + (long long)p * 2 * NSP * g.Kz;
+            cx<T> *st = smc + P * PITCH + (long long)p * 2 * NSP * g.Kz;
 #pragma unroll
             for (int gp = FIRST; gp < 3; gp++) {
 #pragma unroll
@@ -545,7 +546,7 @@ __device__ __forceinline__ void k3_z_body(Geo g, cx<T> *__restrict__ buf, const 
                 else if (pi == FIRST + 2) { cp_async_wait<0>(); __syncthreads(); }
             }
             k3_load_pair<T, L, E>(A, src[pi], false, src[pi + 3], false, g.Kz, sz, q, ok);
-            fft<T, L, E, true, SmPencil<T, L, E>, (32 % (L / E) == 0)>(A, sm, q, tw);
+            pencil_fft<T, L, E, true, (32 % (L / E) == 0)>(A, sm, q, tw);
             if (pi == 0) {
 #pragma unroll
                 for (int e = 0; e < E; e++) { rs[0][e] = A[e].x; rs[1][e] = A[e].y; }
@@ -594,7 +595,7 @@ __device__ __forceinline__ void k3_z_body(Geo g, cx<T> *__restrict__ buf, const 
             const cx<T> *fa = pi < 3 ? F(3 + pi) : pi == 3 ? F(0) : F(2);
             const cx<T> *fb = pi < 3 ? F(6 + pi) : pi == 3 ? F(1) : nullptr;
             k3_load_pair<T, L, E>(A, fa, pi >= 3, fb, pi == 3, g.Kz, sz, q, ok);
-            fft<T, L, E, true, SmPencil<T, L, E>, (32 % (L / E) == 0)>(A, sm, q, tw);
+            pencil_fft<T, L, E, true, (32 % (L / E) == 0)>(A, sm, q, tw);
             switch (pi) {
             case 0:
 #pragma unroll
@@ -720,7 +721,7 @@ __device__ __forceinline__ void k3_z_body(Geo g, cx<T> *__restrict__ buf, const 
         // order the pairs first use them ({u, v}, {w}, {du/dx, du/dy}, {dv/dx, dv/dy},
         // {dw/dx, dw/dy}), so later pairs' loads overlap the earlier transforms.
         // Field f sits in staging slot K3StageSlot(f) of its pencil.
-        cx<T> *const st = reinterpret_cast<cx<T> *>(reinterpret_cast<T *>(smc + P * SmPencil<T, L, E>::PITCH) +
+        cx<T> *const st = reinterpret_cast<cx<T> *>(reinterpret_cast<T *>(smc + P * PITCH) +
                                                     (long long)P * K3Reg<T, MODE, E>::NSM * L) + (long long)p * 9 * g.Kz;
         if constexpr (STAGE) {
 #pragma unroll
@@ -752,7 +753,7 @@ __device__ __forceinline__ void k3_z_body(Geo g, cx<T> *__restrict__ buf, const 
             } else {
                 k3_load_pair<T, L, E>(A, F(fa), pi == 5, F(fb), pi == 1 || pi == 5, g.Kz, sz, q, ok);
             }
-            fft<T, L, E, true, SmPencil<T, L, E>, (32 % (L / E) == 0)>(A, sm, q, tw);
+            pencil_fft<T, L, E, true, (32 % (L / E) == 0)>(A, sm, q, tw);
             switch (pi) {
             case 0:
 #pragma unroll

@@ -78,7 +78,7 @@ constexpr int ZS_WAIT_LIMIT = 1 << 22;
 // pencil, then the block's mbarrier.
 template <typename T, int L, int E, int PB, int SLOTS_SM> struct ZStagedLayout {
     static constexpr int Q = L / E;
-    static constexpr int PITCH = SmPencil<T, L, E>::PITCH;
+    static constexpr int PITCH = pencil_pitch<T, L, E>();
     static constexpr long long SLOT_ELEMS = ((long long)SLOTS_SM * PB * L * (long long)sizeof(T) + (long long)sizeof(cx<T>) - 1) / (long long)sizeof(cx<T>);
     // staging stride of one field: PB*Kz rounded up to 16 bytes
     __host__ __device__ static int stage_stride(int Kz) {
@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(PB *(L / E), MINB) k3_rot_staged(Geo g, cx<T> 
         k3_load_pair<T, L, E>(A, sa, false, sb, false, Kz, sz, q, ok);
         __syncthreads();
         issue(grp, 1, 4);
-        fft<T, L, E, true, SmPencil<T, L, E>, WARP>(A, sm, q, tw);
+        pencil_fft<T, L, E, true, WARP>(A, sm, q, tw);
 #pragma unroll
         for (int e = 0; e < E; e++) { SL(0, e) = A[e].x; SL(2, e) = A[e].y; }
         // pair 1: v + i w_y; then c_z = w_x v - w_y u, transformed and written over w_x (field 3)
@@ -197,14 +197,14 @@ __global__ void __launch_bounds__(PB *(L / E), MINB) k3_rot_staged(Geo g, cx<T> 
         k3_load_pair<T, L, E>(A, sa, false, sb, false, Kz, sz, q, ok);
         __syncthreads();
         issue(grp, 2, 5);
-        fft<T, L, E, true, SmPencil<T, L, E>, WARP>(A, sm, q, tw);
+        pencil_fft<T, L, E, true, WARP>(A, sm, q, tw);
 #pragma unroll
         for (int e = 0; e < E; e++) {
             const T vv = A[e].x, oy = A[e].y;
             SL(1, e) = vv; SL(3, e) = oy;
             A[e] = mk<T>(SL(2, e) * vv - oy * SL(0, e), T(0));
         }
-        fft<T, L, E, false, SmPencil<T, L, E>, WARP>(A, sm, q, tw);
+        pencil_fft<T, L, E, false, WARP>(A, sm, q, tw);
         if (ok) {
             cx<T> *o = FZ(3);
 #pragma unroll
@@ -218,7 +218,7 @@ __global__ void __launch_bounds__(PB *(L / E), MINB) k3_rot_staged(Geo g, cx<T> 
         k3_load_pair<T, L, E>(A, sa, false, sb, false, Kz, sz, q, ok);
         __syncthreads();
         if (grp + gridDim.x < ngrp) issue(grp + gridDim.x, 0, 3);
-        fft<T, L, E, true, SmPencil<T, L, E>, WARP>(A, sm, q, tw);
+        pencil_fft<T, L, E, true, WARP>(A, sm, q, tw);
 #pragma unroll
         for (int e = 0; e < E; e++) {
             const T ww = A[e].x, oz = A[e].y, uu = SL(0, e), vv = SL(1, e);
@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(PB *(L / E), MINB) k3_rot_staged(Geo g, cx<T> 
             A[e] = mk<T>(SL(3, e) * ww - oz * vv, oz * uu - SL(2, e) * ww);
         }
         // forward transform of c_x + i c_y and extraction of both half spectra, kz < Kz
-        fft<T, L, E, false, SmPencil<T, L, E>, WARP>(A, sm, q, tw);
+        pencil_fft<T, L, E, false, WARP>(A, sm, q, tw);
 #pragma unroll
         for (int e = 0; e < E; e++) sm.at(out_row<L, E, false>(q, e)) = A[e];
         stage_barrier<WARP>();

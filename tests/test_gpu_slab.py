@@ -84,3 +84,40 @@ def test_slab_rejects_what_it_cannot_do():
         SlabRank(make_args(32, conj=True), 2, 0)
     with pytest.raises(SpnsError):
         SlabRank(make_args(32), 40, 0)        # 33 ky rows cannot give 40 ranks a row each
+
+
+def test_torch_transport_one_rank_over_nccl():
+    """The multi-process transport (torch.distributed over NCCL) with one rank: the slab
+    phases, the all-to-all calls on the rank's stream and the reductions run through NCCL
+    on the GPU, and the step equals the one-GPU step."""
+    import os
+    import socket
+    import torch
+    import torch.distributed as dist
+    from spns_b200.hit import HIT
+    from spns_b200.slab import SlabHIT, TorchTransport
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    os.environ["MASTER_ADDR"], os.environ["MASTER_PORT"] = "127.0.0.1", str(port)
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", rank=0, world_size=1, device_id=torch.device("cuda", 0))
+    try:
+        box = (32, 32, 32)
+        args = make_args(0, nu=3.283e-4, Ns=box, self_adaptive=True)
+        one = HIT(args, nonlinear_form=2, eps_forcing=0.1)
+        slab = SlabHIT(args, 1, TorchTransport(), ranks=[0], eps_forcing=0.1)
+        U0 = broadband_field(*box, seed=4)
+        for h in (one, slab):
+            h.set_compact(U0)
+            h.Recalculate_Velocity_Antitransform()
+            h.Recalculate_TimeStep()
+        one.New_Fractional_Step_Method(10)
+        slab.New_Fractional_Step_Method(10)
+        torch.cuda.synchronize()
+        assert rel_l2(slab.get_compact(), one.get_compact()) < 1e-12
+        assert abs(slab.getAt() - one.getAt()) <= 1e-13 * one.getAt()
+        slab.close()
+        one.close()
+    finally:
+        dist.destroy_process_group()
