@@ -1177,6 +1177,32 @@ template <typename T> __device__ __forceinline__ cx<double> load_state(const cx<
     return r;
 }
 
+// Adds each lane's e (and o, when hO is given) to the bins hE[K] (hO[K]) in shared
+// memory, K < 0 adding nothing.  Called by all 32 lanes with K non-decreasing in the
+// lane (32 consecutive kz of one row): the lanes of one shell are then contiguous,
+// a segmented scan over the runs of equal K (five shuffle steps) leaves each run's
+// sum in its last lane, and those lanes add to distinct bins in one atomic
+// instruction.  (Consecutive kz fall in different shells about every other mode,
+// so per-lane atomics would collide on few bins and a loop over the warp's shells
+// would run about twenty rounds.)  Lanes out of order only cost extra atomics.
+__device__ __forceinline__ void warp_shell_add(int K, double e, double o, double *hE, double *hO) {
+    const int lane = threadIdx.x & 31;
+    const int Kprev = __shfl_up_sync(0xffffffffu, K, 1);
+    const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || Kprev != K);
+    const int start = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));   // first lane of this lane's run
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const double te = __shfl_up_sync(0xffffffffu, e, off);
+        const double to = hO ? __shfl_up_sync(0xffffffffu, o, off) : 0.0;
+        if (lane - off >= start) { e += te; o += to; }
+    }
+    const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
+    if (tail && K >= 0) {
+        atomicAdd(&hE[K], e);
+        if (hO) atomicAdd(&hO[K], o);
+    }
+}
+
 template <typename T>
 __global__ void k_shell_sums(Geo g, const cx<T> *__restrict__ u, const cx<T> *__restrict__ v, const cx<T> *__restrict__ w,
                              const cx<T> *__restrict__ ulo, const cx<T> *__restrict__ vlo, const cx<T> *__restrict__ wlo,
@@ -1185,22 +1211,40 @@ __global__ void k_shell_sums(Geo g, const cx<T> *__restrict__ u, const cx<T> *__
     double *hE = hist, *hO = hist + (Kmax + 1);
     for (int i = threadIdx.x; i < 2 * (Kmax + 1); i += blockDim.x) hist[i] = 0.0;
     __syncthreads();
-    const long long n = g.S0;
-    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long long)gridDim.x * blockDim.x) {
-        const int kz = (int)(idx % g.Kz);
-        const long long t = idx / g.Kz;
-        const int ix = (int)(t % g.Kx), iy = (int)(t / g.Kx);
+    const int lane = threadIdx.x & 31;
+    // One warp per row (iy, ix) of Kz modes, the lanes along kz: the row's k1^2 + k2^2
+    // and offset are computed once, the loads of a warp are 32 consecutive modes, and
+    // K grows with kz along the row, so a warp's 32 modes fall in one to three shells
+    // and the lanes combine their contributions per shell before one lane adds them
+    // (shared-memory atomics of a warp on one bin serialise).
+    const int rows = g.Ky * g.Kx;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < rows; row += nw) {
+        const int ix = row % g.Kx, iy = row / g.Kx;
         const long long k1 = (long long)g.sx * (ix <= g.hx ? ix : ix - g.Kx);
         const long long k2 = (long long)g.sy * ky_mode(g, iy);
-        const long long k3 = (long long)g.sz * kz;
-        const double rad2 = (double)(k1 * k1 + k2 * k2 + k3 * k3);
-        const int K = (int)round(sqrt(rad2));
-        if (K > Kmax) continue;
-        const cx<double> a = load_state(u, ulo, idx), b = load_state(v, vlo, idx), cc = load_state(w, wlo, idx);
-        double e = 0.5 * (a.x * a.x + a.y * a.y + b.x * b.x + b.y * b.y + cc.x * cc.x + cc.y * cc.y);
-        if (kz != 0) e *= 2.0;
-        atomicAdd(&hE[K], e);
-        atomicAdd(&hO[K], 2.0 * rad2 * e);
+        const long long r12 = k1 * k1 + k2 * k2;
+        const long long rb = (long long)row * g.Kz;
+        for (int kz0 = 0; kz0 < g.Kz; kz0 += 32) {
+            const int kz = kz0 + lane;
+            int K = -1;
+            double e = 0.0, o = 0.0;
+            if (kz < g.Kz) {
+                const long long k3 = (long long)g.sz * kz;
+                const double rad2 = (double)(r12 + k3 * k3);
+                K = (int)round(sqrt(rad2));
+                if (K <= Kmax) {
+                    const long long idx = rb + kz;
+                    const cx<double> a = load_state(u, ulo, idx), b = load_state(v, vlo, idx), cc = load_state(w, wlo, idx);
+                    e = 0.5 * (a.x * a.x + a.y * a.y + b.x * b.x + b.y * b.y + cc.x * cc.x + cc.y * cc.y);
+                    if (kz != 0) e *= 2.0;
+                    o = 2.0 * rad2 * e;
+                } else {
+                    K = -1;
+                }
+            }
+            warp_shell_add(K, e, o, hE, hO);
+        }
     }
     __syncthreads();
     for (int i = threadIdx.x; i <= Kmax; i += blockDim.x) {
@@ -1217,20 +1261,33 @@ __global__ void k_shell_sums_scalar(Geo g, const cx<T> *__restrict__ F, double s
     extern __shared__ double hist[];
     for (int i = threadIdx.x; i <= Kmax; i += blockDim.x) hist[i] = 0.0;
     __syncthreads();
-    const long long n = g.S0;
-    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long long)gridDim.x * blockDim.x) {
-        const int kz = (int)(idx % g.Kz);
-        const long long t = idx / g.Kz;
-        const int ix = (int)(t % g.Kx), iy = (int)(t / g.Kx);
+    // one warp per row (iy, ix), the lanes along kz, as in k_shell_sums
+    const int lane = threadIdx.x & 31;
+    const int rows = g.Ky * g.Kx;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < rows; row += nw) {
+        const int ix = row % g.Kx, iy = row / g.Kx;
         const long long k1 = (long long)g.sx * (ix <= g.hx ? ix : ix - g.Kx);
         const long long k2 = (long long)g.sy * ky_mode(g, iy);
-        const long long k3 = (long long)g.sz * kz;
-        const int K = (int)round(sqrt((double)(k1 * k1 + k2 * k2 + k3 * k3)));
-        if (K > Kmax) continue;
-        const cx<T> a = F[idx];
-        double e = scale * ((double)a.x * a.x + (double)a.y * a.y);
-        if (kz != 0) e *= 2.0;
-        atomicAdd(&hist[K], e);
+        const long long r12 = k1 * k1 + k2 * k2;
+        const long long rb = (long long)row * g.Kz;
+        for (int kz0 = 0; kz0 < g.Kz; kz0 += 32) {
+            const int kz = kz0 + lane;
+            int K = -1;
+            double e = 0.0;
+            if (kz < g.Kz) {
+                const long long k3 = (long long)g.sz * kz;
+                K = (int)round(sqrt((double)(r12 + k3 * k3)));
+                if (K <= Kmax) {
+                    const cx<T> a = F[rb + kz];
+                    e = scale * ((double)a.x * a.x + (double)a.y * a.y);
+                    if (kz != 0) e *= 2.0;
+                } else {
+                    K = -1;
+                }
+            }
+            warp_shell_add(K, e, 0.0, hist, nullptr);
+        }
     }
     __syncthreads();
     for (int i = threadIdx.x; i <= Kmax; i += blockDim.x)
