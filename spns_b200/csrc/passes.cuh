@@ -265,7 +265,7 @@ template <typename T> struct Passes {
         const int nb = h->last_rad_max + 1;
         CK(cudaMemsetAsync(h->bins, 0, sizeof(double) * 2 * nb, h->st));
         const long long n = h->g.S0;
-        const int blocks = (int)std::min<long long>((n + 255) / 256, 8LL * h->sms);
+        const int blocks = (int)std::min<long long>((n + 255) / 256, (long long)spns::SHELL_BLOCKS_PER_SM * h->sms);
         spns::k_shell_sums<T><<<blocks, 256, sizeof(double) * 2 * nb, h->st>>>(h->g, U(h, 0), U(h, 1), U(h, 2), Ulo(h, 0), Ulo(h, 1),
                                                                               Ulo(h, 2), h->last_rad_max, h->bins, h->bins + nb);
         CKL();
@@ -327,7 +327,7 @@ template <typename T> struct Passes {
         if (r) return r;
         CK(cudaMemsetAsync(h->inv_bins, 0, sizeof(double) * 5 * nb, h->st));
         const double scale = h->c.inv_norm * h->c.inv_norm;
-        const int blocks = (int)std::min<long long>((g.S0 + 255) / 256, 8LL * h->sms);
+        const int blocks = (int)std::min<long long>((g.S0 + 255) / 256, (long long)spns::SHELL_BLOCKS_PER_SM * h->sms);
         for (int c = 0; c < 5; c++) {
             spns::k_shell_sums_scalar<T><<<blocks, 256, sizeof(double) * nb, h->st>>>(
                 g, (const C *)h->inv_B2 + (long long)c * g.S0, scale, h->last_rad_max, h->inv_bins + (long long)c * nb);

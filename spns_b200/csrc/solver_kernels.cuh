@@ -1179,7 +1179,7 @@ template <typename T> __device__ __forceinline__ cx<double> load_state(const cx<
 
 // Adds each lane's e (and o, when hO is given) to the bins hE[K] (hO[K]) in shared
 // memory, K < 0 adding nothing.  Called by all 32 lanes with K non-decreasing in the
-// lane (32 consecutive kz of one row): the lanes of one shell are then contiguous,
+// lane (consecutive kz of one row): the lanes of one shell are then contiguous,
 // a segmented scan over the runs of equal K (five shuffle steps) leaves each run's
 // sum in its last lane, and those lanes add to distinct bins in one atomic
 // instruction.  (Consecutive kz fall in different shells about every other mode,
@@ -1203,49 +1203,69 @@ __device__ __forceinline__ void warp_shell_add(int K, double e, double o, double
     }
 }
 
+// Walks this warp's share of the compact modes 32 at a time: a contiguous run of whole
+// rows (iy, ix), flattened, so that every round but the last is 32 consecutive modes
+// (coalesced loads, no idle lanes at the end of a row of Kz modes).  Calls
+// f(valid, idx, kz, r12) on all 32 lanes each round, r12 = (sx m1)^2 + (sy m2)^2 of
+// the lane's row (recomputed only when the lane enters a new row).  Along a row K
+// grows with kz, so a round's lanes form runs of equal K, as warp_shell_add wants.
+template <typename F> __device__ __forceinline__ void warp_mode_rounds(const Geo &g, F &&f) {
+    const int lane = threadIdx.x & 31;
+    const int rows = g.Ky * g.Kx;
+    const int nw = (gridDim.x * blockDim.x) >> 5, wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int per = (rows + nw - 1) / nw;
+    const int r0 = (int)min((long long)wid * per, (long long)rows), r1 = min(rows, r0 + per);
+    const long long end = (long long)r1 * g.Kz;
+    int row = r0, kz = lane;
+    while (kz >= g.Kz) { kz -= g.Kz; row++; }
+    int crow = -1;
+    long long r12 = 0;
+    for (long long base = (long long)r0 * g.Kz; base < end; base += 32) {
+        const long long idx = base + lane;
+        const bool valid = idx < end;
+        if (valid && row != crow) {
+            crow = row;
+            const int ix = row % g.Kx, iy = row / g.Kx;
+            const long long k1 = (long long)g.sx * (ix <= g.hx ? ix : ix - g.Kx);
+            const long long k2 = (long long)g.sy * ky_mode(g, iy);
+            r12 = k1 * k1 + k2 * k2;
+        }
+        f(valid, idx, kz, r12);
+        kz += 32;
+        while (kz >= g.Kz) { kz -= g.Kz; row++; }
+    }
+}
+
+// Shell-sum kernels: 256 threads, at most 42 registers, so six blocks fill an SM
+// and a grid of SHELL_BLOCKS_PER_SM blocks per SM is one wave.
+constexpr int SHELL_BLOCKS_PER_SM = 6;
+
 template <typename T>
-__global__ void k_shell_sums(Geo g, const cx<T> *__restrict__ u, const cx<T> *__restrict__ v, const cx<T> *__restrict__ w,
+__global__ void __launch_bounds__(256, SHELL_BLOCKS_PER_SM) k_shell_sums(Geo g, const cx<T> *__restrict__ u, const cx<T> *__restrict__ v, const cx<T> *__restrict__ w,
                              const cx<T> *__restrict__ ulo, const cx<T> *__restrict__ vlo, const cx<T> *__restrict__ wlo,
                              int Kmax, double *__restrict__ Ek, double *__restrict__ Om) {
     extern __shared__ double hist[];
     double *hE = hist, *hO = hist + (Kmax + 1);
     for (int i = threadIdx.x; i < 2 * (Kmax + 1); i += blockDim.x) hist[i] = 0.0;
     __syncthreads();
-    const int lane = threadIdx.x & 31;
-    // One warp per row (iy, ix) of Kz modes, the lanes along kz: the row's k1^2 + k2^2
-    // and offset are computed once, the loads of a warp are 32 consecutive modes, and
-    // K grows with kz along the row, so a warp's 32 modes fall in one to three shells
-    // and the lanes combine their contributions per shell before one lane adds them
-    // (shared-memory atomics of a warp on one bin serialise).
-    const int rows = g.Ky * g.Kx;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < rows; row += nw) {
-        const int ix = row % g.Kx, iy = row / g.Kx;
-        const long long k1 = (long long)g.sx * (ix <= g.hx ? ix : ix - g.Kx);
-        const long long k2 = (long long)g.sy * ky_mode(g, iy);
-        const long long r12 = k1 * k1 + k2 * k2;
-        const long long rb = (long long)row * g.Kz;
-        for (int kz0 = 0; kz0 < g.Kz; kz0 += 32) {
-            const int kz = kz0 + lane;
-            int K = -1;
-            double e = 0.0, o = 0.0;
-            if (kz < g.Kz) {
-                const long long k3 = (long long)g.sz * kz;
-                const double rad2 = (double)(r12 + k3 * k3);
-                K = (int)round(sqrt(rad2));
-                if (K <= Kmax) {
-                    const long long idx = rb + kz;
-                    const cx<double> a = load_state(u, ulo, idx), b = load_state(v, vlo, idx), cc = load_state(w, wlo, idx);
-                    e = 0.5 * (a.x * a.x + a.y * a.y + b.x * b.x + b.y * b.y + cc.x * cc.x + cc.y * cc.y);
-                    if (kz != 0) e *= 2.0;
-                    o = 2.0 * rad2 * e;
-                } else {
-                    K = -1;
-                }
+    warp_mode_rounds(g, [&](bool valid, long long idx, int kz, long long r12) {
+        int K = -1;
+        double e = 0.0, o = 0.0;
+        if (valid) {
+            const long long k3 = (long long)g.sz * kz;
+            const double rad2 = (double)(r12 + k3 * k3);
+            K = (int)round(sqrt(rad2));
+            if (K <= Kmax) {
+                const cx<double> a = load_state(u, ulo, idx), b = load_state(v, vlo, idx), cc = load_state(w, wlo, idx);
+                e = 0.5 * (a.x * a.x + a.y * a.y + b.x * b.x + b.y * b.y + cc.x * cc.x + cc.y * cc.y);
+                if (kz != 0) e *= 2.0;
+                o = 2.0 * rad2 * e;
+            } else {
+                K = -1;
             }
-            warp_shell_add(K, e, o, hE, hO);
         }
-    }
+        warp_shell_add(K, e, o, hE, hO);
+    });
     __syncthreads();
     for (int i = threadIdx.x; i <= Kmax; i += blockDim.x) {
         if (hE[i] != 0.0) atomicAdd(&Ek[i], hE[i]);
@@ -1257,38 +1277,26 @@ __global__ void k_shell_sums(Geo g, const cx<T> *__restrict__ u, const cx<T> *__
 // spectrum of one scalar field (src/HIT_LES.cpp:1137-1214 with the integrands of
 // the invariant spectra, :1006-1025).
 template <typename T>
-__global__ void k_shell_sums_scalar(Geo g, const cx<T> *__restrict__ F, double scale, int Kmax, double *__restrict__ out) {
+__global__ void __launch_bounds__(256, SHELL_BLOCKS_PER_SM) k_shell_sums_scalar(Geo g, const cx<T> *__restrict__ F, double scale, int Kmax, double *__restrict__ out) {
     extern __shared__ double hist[];
     for (int i = threadIdx.x; i <= Kmax; i += blockDim.x) hist[i] = 0.0;
     __syncthreads();
-    // one warp per row (iy, ix), the lanes along kz, as in k_shell_sums
-    const int lane = threadIdx.x & 31;
-    const int rows = g.Ky * g.Kx;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < rows; row += nw) {
-        const int ix = row % g.Kx, iy = row / g.Kx;
-        const long long k1 = (long long)g.sx * (ix <= g.hx ? ix : ix - g.Kx);
-        const long long k2 = (long long)g.sy * ky_mode(g, iy);
-        const long long r12 = k1 * k1 + k2 * k2;
-        const long long rb = (long long)row * g.Kz;
-        for (int kz0 = 0; kz0 < g.Kz; kz0 += 32) {
-            const int kz = kz0 + lane;
-            int K = -1;
-            double e = 0.0;
-            if (kz < g.Kz) {
-                const long long k3 = (long long)g.sz * kz;
-                K = (int)round(sqrt((double)(r12 + k3 * k3)));
-                if (K <= Kmax) {
-                    const cx<T> a = F[rb + kz];
-                    e = scale * ((double)a.x * a.x + (double)a.y * a.y);
-                    if (kz != 0) e *= 2.0;
-                } else {
-                    K = -1;
-                }
+    warp_mode_rounds(g, [&](bool valid, long long idx, int kz, long long r12) {
+        int K = -1;
+        double e = 0.0;
+        if (valid) {
+            const long long k3 = (long long)g.sz * kz;
+            K = (int)round(sqrt((double)(r12 + k3 * k3)));
+            if (K <= Kmax) {
+                const cx<T> a = F[idx];
+                e = scale * ((double)a.x * a.x + (double)a.y * a.y);
+                if (kz != 0) e *= 2.0;
+            } else {
+                K = -1;
             }
-            warp_shell_add(K, e, 0.0, hist, nullptr);
         }
-    }
+        warp_shell_add(K, e, 0.0, hist, nullptr);
+    });
     __syncthreads();
     for (int i = threadIdx.x; i <= Kmax; i += blockDim.x)
         if (hist[i] != 0.0) atomicAdd(&out[i], hist[i]);

@@ -106,7 +106,7 @@ extern "C" int spns_energy_cascade_noalloc_f64(const void *uvw_dev, int Kx, int 
     e = cudaMemsetAsync(bins, 0, sizeof(double) * 2 * (size_t)nbins, st);
     if (e != cudaSuccess) return noalloc_fail(SPNS_ERR_CUDA, cudaGetErrorString(e));
     const long long n = g.S0;
-    const long long cap = 8LL * sms;   // 8 resident blocks of 256 threads per SM
+    const long long cap = (long long)SHELL_BLOCKS_PER_SM * sms;   // one wave of resident blocks
     const int blocks = (int)((n + 255) / 256 < cap ? (n + 255) / 256 : cap);
     k_shell_sums<double><<<blocks, 256, sizeof(double) * 2 * nbins, st>>>(
         g, (const cx<double> *)u, (const cx<double> *)(u + g.S0), (const cx<double> *)(u + 2 * g.S0), nullptr, nullptr, nullptr, nbins - 1, bins,
