@@ -11,10 +11,12 @@ C_At=0.5, FP64 plain form.  A "step" is one HIT::New_Fractional_Step_Method.
 the solver has no data-path collective, so `value` is the sum over ranks
 (N*K steps / max over ranks of the device time) and scaling is weak.
 
---impl reference times the reference algorithm on the host cores (the CPU
-oracle, a C restatement of the reference solver with OpenMP threads in its
-FFTs, as FFTW threads are in the reference) on a bounded sample of the same
-workload, and prints the same JSON line with "impl": "reference".
+--impl reference times the reference solver on the host cores (oracle/_ref:
+src/*.cpp of adalbal/SpNS compiled unchanged against single-process MPI and
+FFTW stand-ins, the oracle's OpenMP FFT in place of FFTW's threads; where it
+was not built, the CPU oracle, a C restatement of the same solver) on a bounded
+sample of the same workload, and prints the same JSON line with
+"impl": "reference".
 """
 from __future__ import annotations
 
@@ -192,19 +194,63 @@ def cpu_sample(n_sample: int, steps: int, threads: int):
     return (time.perf_counter() - t0) / steps
 
 
+REF_EXE = os.path.join(ROOT, "oracle", "_ref", "spns_ref")
+
+
+def ref_run(workdir: str, n: int, final_time: float, threads: int):
+    """One run of the compiled reference solver on an n^3 box: (wall s, steps, final time)."""
+    with open(os.path.join(workdir, "params"), "w") as fh:
+        fh.write(f"Nx\t{n}\nNy\t{n}\nNz\t{n}\nnu\t{nu_for(N_BOX):.6e}\nFinal_Time\t{final_time:.9e}\n"
+                 f"C_At\t0.5\nSelfAdaptiveTimestep\t1\nOMP_Threads\t{threads}\n")
+    t0 = time.perf_counter()
+    r = subprocess.run([REF_EXE, "params"], cwd=workdir, capture_output=True, timeout=1800)
+    wall = time.perf_counter() - t0
+    out = r.stdout.decode(errors="replace")
+    if r.returncode != 0:
+        raise RuntimeError(f"reference solver failed ({r.returncode}): {out[-500:]}")
+    import re
+    steps = int(re.search(r"Final time-steps:\s*(\d+)", out).group(1))
+    t_end = float(re.search(r"Final time:\s*(\S+)", out).group(1))
+    return wall, steps, t_end
+
+
+def ref_sample(n_sample: int, steps: int, threads: int):
+    """Seconds per step of the compiled reference solver at N=n_sample: a one-step run and a
+    run of about 1 + `steps` steps, both timed whole; their difference cancels the set-up
+    (K41 field, allocation, planning).  Returns (s/step, steps timed)."""
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        w1, n1, dt1 = ref_run(d, n_sample, 1e-12, threads)
+        w2, n2, _ = ref_run(d, n_sample, dt1 * (steps + 1.5), threads)
+    if n2 <= n1:
+        raise RuntimeError("reference sample ran no extra step")
+    return (w2 - w1) / (n2 - n1), n2 - n1
+
+
+def cpu_step_seconds(n_sample: int, steps: int, threads: int):
+    """(s/step, kind, description) of the CPU reference at N=n_sample: the compiled
+    reference solver where it was built, else the oracle port."""
+    if os.path.exists(REF_EXE):
+        s, k = ref_sample(n_sample, steps, threads)
+        return s, "reference", (f"the reference solver (src/*.cpp compiled unchanged; MPI/FFTW stand-ins, the oracle's "
+                                f"OpenMP FFT in place of FFTW) at N={n_sample}, {k} steps timed, {s:.3f} s/step; "
+                                f"unforced (its eps-forcing block is disabled), K41 initial field, same nu and kappa scheme")
+    s = cpu_sample(n_sample, steps, threads)
+    return s, "port", f"{steps} steps of the CPU oracle (C restatement) at N={n_sample}, {s:.3f} s/step"
+
+
 def fft_work(N: int) -> float:
     M = (3 * N) // 2
     return M ** 3 * math.log2(M ** 3)
 
 
 def cpu_baseline_block(threads: int, n_sample: int = 96, steps: int = 3):
-    s = cpu_sample(n_sample, steps, threads)
+    s, kind, desc = cpu_step_seconds(n_sample, steps, threads)
     scale = fft_work(N_BOX) / fft_work(n_sample)
     v = 1.0 / (s * scale)
-    return {"value": v, "unit": "steps/s", "cores": threads, "kind": "port",
-            "sample": (f"{steps} steps of the same forced DNS at N={n_sample} (FFT {(3 * n_sample) // 2}^3), "
-                       f"{s:.3f} s/step, extrapolated to N={N_BOX} by FFT work M^3 log2 M^3 (x{scale:.1f}); "
-                       f"the reference layout needs ~200 GB of host RAM at N={N_BOX}")}
+    return {"value": v, "unit": "steps/s", "cores": threads, "kind": kind,
+            "sample": (f"{desc} (FFT {(3 * n_sample) // 2}^3), extrapolated to N={N_BOX} by FFT work "
+                       f"M^3 log2 M^3 (x{scale:.1f}); the reference layout needs ~200 GB of host RAM at N={N_BOX}")}
 
 
 def _timed_steps(h, n: int) -> float:
@@ -287,7 +333,7 @@ def same_n_block(local: int, n: int, threads: int, cpu_steps: int = 3, gpu_steps
     from spns_b200.hit import HIT
     from spns_b200.fields import seeded_spectral_field
     import torch
-    s_cpu = cpu_sample(n, cpu_steps, threads)
+    s_cpu, kind, desc = cpu_step_seconds(n, cpu_steps, threads)
     a = box_args(n)
     a.nu = nu_for(N_BOX)
     h = HIT(a, device=local, eps_forcing=EPS)
@@ -309,7 +355,7 @@ def same_n_block(local: int, n: int, threads: int, cpu_steps: int = 3, gpu_steps
         h.Recalculate_Energy_Cascade()
     e2e_s = (time.perf_counter() - t0) / gpu_steps
     h.close()
-    return {"N": n, "fft_grid": (3 * n) // 2, "cores": threads, "kind": "port",
+    return {"N": n, "fft_grid": (3 * n) // 2, "cores": threads, "kind": kind, "cpu_sample": desc,
             "cpu_steps": cpu_steps, "cpu_steps_per_s": 1.0 / s_cpu,
             "gpu_steps": gpu_steps, "gpu_steps_per_s": 1.0 / gpu_s, "gpu_e2e_steps_per_s": 1.0 / e2e_s,
             "gpu_over_cpu": s_cpu / gpu_s, "gpu_e2e_over_cpu": s_cpu / e2e_s,
@@ -457,12 +503,17 @@ def run_reference(args):
         return 0
     threads = os.cpu_count() or 1
     n_sample = args.ref_sample_n
-    for _ in range(args.warmup):
-        cpu_sample(n_sample, 1, threads)
-    per = []
-    for _ in range(max(1, args.steps)):
-        per.append(cpu_sample(n_sample, 1, threads))
-    s = sum(per) / len(per)
+    if os.path.exists(REF_EXE):
+        # W warm-up steps inside the first (set-up cancelling) run pair, then K timed steps
+        if args.warmup > 0:
+            ref_sample(n_sample, args.warmup, threads)
+        s, kind, desc = cpu_step_seconds(n_sample, max(1, args.steps), threads)
+    else:
+        for _ in range(args.warmup):
+            cpu_sample(n_sample, 1, threads)
+        per = [cpu_sample(n_sample, 1, threads) for _ in range(max(1, args.steps))]
+        s, kind = sum(per) / len(per), "port"
+        desc = f"one CPU-oracle step at N={n_sample} per timed step, {s:.3f} s/step"
     scale = fft_work(N_BOX) / fft_work(n_sample)
     value = 1.0 / (s * scale)
     line = {
@@ -471,8 +522,8 @@ def run_reference(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"forced DNS N={N_BOX} (FFT 768^3), eps=0.1 on K=1..2, self-adaptive dt",
                    "sample": f"N={n_sample} per step, extrapolated"},
-        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": "port",
-                         "sample": f"one oracle step at N={n_sample} per timed step, {s:.3f} s, x{scale:.1f} FFT work to N={N_BOX}"},
+        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": kind,
+                         "sample": f"{desc}; x{scale:.1f} FFT work to N={N_BOX}"},
         "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
