@@ -24,6 +24,7 @@ import argparse
 import json
 import math
 import os
+import re
 import subprocess
 import sys
 import time
@@ -208,7 +209,6 @@ def ref_run(workdir: str, n: int, final_time: float, threads: int):
     out = r.stdout.decode(errors="replace")
     if r.returncode != 0:
         raise RuntimeError(f"reference solver failed ({r.returncode}): {out[-500:]}")
-    import re
     steps = int(re.search(r"Final time-steps:\s*(\d+)", out).group(1))
     t_end = float(re.search(r"Final time:\s*(\S+)", out).group(1))
     return wall, steps, t_end
