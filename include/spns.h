@@ -304,7 +304,8 @@ const char *spns_status_string(int status);
  * above SPNS_NOALLOC_MAX_BINS is rejected with SPNS_ERR_UNSUPPORTED_SIZE.  The
  * first call on a device looks up the array's device address and the device's
  * SM count (cudaGetSymbolAddress, cudaDeviceGetAttribute) and keeps them for
- * the life of the process: do not call it after cudaDeviceReset on that
+ * the life of the process: make that first call before any stream capture is
+ * under way on the device, and do not call it after cudaDeviceReset on that
  * device.  All calls share the array: calls whose GPU work overlaps race and
  * must be serialised by the caller.  Error text: spns_last_error(NULL). */
 #define SPNS_NOALLOC_MAX_BINS 2048

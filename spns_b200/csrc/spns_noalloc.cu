@@ -18,9 +18,10 @@
 // it keeps the contents of the last call, so each call clears it first; calls
 // whose work overlaps on the GPU (different streams, or different host threads
 // on one device) race on it and must be serialised by the caller.  The array's
-// device address and the device's SM count are looked up once per device and
-// kept for the life of the process, so the entry point must not be used after
-// the host program calls cudaDeviceReset on that device.
+// device address and the device's SM count are looked up by the first call on
+// each device and kept for the life of the process: that first call should come
+// before any stream capture is under way on the device, and the entry point must
+// not be used after the host program calls cudaDeviceReset on that device.
 #include "spns.h"
 #include "solver_kernels.cuh"
 
