@@ -16,7 +16,13 @@
 // Radices 2, 3, 4, 6, 8, 12: the composite ones with a factor 3 use the
 // prime-factor (Good-Thomas) split 2x3 / 4x3, which needs no inner twiddles.
 // Twiddles: w^1 of a butterfly is read from a table w_L^m = exp(-2 pi i m/L)
-// computed on the host in extended precision.  In double precision its powers
+// computed on the host in extended precision.  Stage (R, Ns) needs w_L^{r k L/(Ns R)}
+// = w_n^{r k} with n = Ns R and k = j mod Ns; the table carries, after its L base
+// entries, a copy w_n^m of the base values for every divisor n < L of L
+// (tw_sub_offset), so the lanes of a warp (consecutive k) read consecutive
+// entries instead of entries L/n apart: one or two L1 wavefronts per warp load
+// instead of up to 32 lines.  The values are the same table entries, so results
+// do not change.  In double precision its powers
 // w^r are formed by repeated complex multiplication (one table read per
 // butterfly instead of R-1: the table reads contend with the shared-memory
 // exchange for the load/store pipe); in single precision, where a chain of up
@@ -172,6 +178,24 @@ template <class SM, bool INV, int S> __host__ __device__ constexpr int ex_pad() 
     else return 0;
 }
 
+// Offset of the sub-table w_n^m (m < n) in a twiddle table of length L: 0 for
+// n = L (the base table), else L plus the sizes of the sub-tables of the divisors
+// of L below n (spns_make_twiddles lays them out in increasing n).
+__host__ __device__ constexpr int tw_sub_offset(int L, int n) {
+    if (n >= L) return 0;
+    int off = L;
+    for (int d = 2; d < n; d++)
+        if (L % d == 0) off += d;
+    return off;
+}
+// Entries of a twiddle table of length L with all its sub-tables.
+__host__ __device__ constexpr int tw_table_size(int L) {
+    int s = L;
+    for (int d = 2; d < L; d++)
+        if (L % d == 0) s += d;
+    return s;
+}
+
 template <bool WARP> __device__ __forceinline__ void stage_barrier() {
     if constexpr (WARP) __syncwarp(); else __syncthreads();
 }
@@ -209,15 +233,16 @@ __device__ __forceinline__ void fft_run(cx<T> (&v)[E], SM sm, int q, const cx<T>
     for (int m = 0; m < MB; m++) {
         if constexpr (Ns > 1) {
             const int j = q + Q * m;
-            const int k = j % Ns;
-            const int step = k * (L / (Ns * R));   // r*step < L for r < R
+            const int k = j % Ns;                  // w^r = w_n^{r k}, n = Ns R, r k < n
+            constexpr int TWO = tw_sub_offset(L, Ns * R);
+            const cx<T> *__restrict__ twn = tw + TWO;
             if constexpr (sizeof(T) == 4) {
                 cx<T> wp[R];
-                twiddle_powers<T, R>(wp, tw, step);
+                twiddle_powers<T, R>(wp, twn, k);
 #pragma unroll
                 for (int r = 1; r < R; r++) v[m * R + r] = INV ? cmulc(v[m * R + r], wp[r]) : cmul(v[m * R + r], wp[r]);
             } else {
-                const cx<T> w1 = tw[step];
+                const cx<T> w1 = twn[k];
                 cx<T> w = w1;
 #pragma unroll
                 for (int r = 1; r < R; r++) {

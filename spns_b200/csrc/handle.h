@@ -310,18 +310,26 @@ int spns_fail(spns_handle *h, int code, const char *fmt, ...);
     default: return spns_fail(h, SPNS_ERR_UNSUPPORTED_SIZE, "FFT length %d is not compiled", Lval); \
     }
 
-// Twiddle table w_L^m = exp(-2 pi i m / L), computed in extended precision;
-// allocated in stream order on `st` (no device-wide synchronisation).
+// Twiddle table w_L^m = exp(-2 pi i m / L), computed in extended precision, followed
+// by the per-stage sub-tables w_n^m = w_L^{m L/n} (copies of base entries) for every
+// divisor n < L of L, in increasing n (spns::tw_sub_offset); allocated in stream
+// order on `st` (no device-wide synchronisation).
 template <typename T> inline void *spns_make_twiddles(int L, cudaStream_t st) {
-    std::vector<spns::cx<T>> t(L);
+    const int total = spns::tw_table_size(L);
+    std::vector<spns::cx<T>> t(total);
     for (int m = 0; m < L; m++) {
         long double ang = 2.0L * 3.14159265358979323846264338327950288L * (long double)m / (long double)L;
         t[m].x = (T)cosl(ang);
         t[m].y = (T)(-sinl(ang));
     }
+    for (int n = 2; n < L; n++) {
+        if (L % n) continue;
+        const int off = spns::tw_sub_offset(L, n);
+        for (int m = 0; m < n; m++) t[off + m] = t[(long long)m * (L / n)];
+    }
     void *d = nullptr;
-    if (cudaMallocAsync(&d, sizeof(spns::cx<T>) * L, st) != cudaSuccess) return nullptr;
-    if (cudaMemcpyAsync(d, t.data(), sizeof(spns::cx<T>) * L, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+    if (cudaMallocAsync(&d, sizeof(spns::cx<T>) * total, st) != cudaSuccess) return nullptr;
+    if (cudaMemcpyAsync(d, t.data(), sizeof(spns::cx<T>) * total, cudaMemcpyHostToDevice, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess) {
         cudaFreeAsync(d, st);
         return nullptr;
