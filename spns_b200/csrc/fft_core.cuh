@@ -195,6 +195,18 @@ __host__ __device__ constexpr int tw_table_size(int L) {
         if (L % d == 0) s += d;
     return s;
 }
+// Single precision reads the powers of two of a butterfly's twiddle; w_n^{r k} for
+// r = 2, 4, 8 sits in a power table of its own (n entries, k contiguous) so that those
+// reads are contiguous across a warp too.  Three power tables follow the sub-tables,
+// each holding every divisor n >= 2 of L (L included) in increasing n.
+__host__ __device__ constexpr int tw_pow_offset(int L, int n, int r) {
+    const int ri = r == 2 ? 0 : r == 4 ? 1 : 2;
+    int off = tw_table_size(L) * (1 + ri);
+    for (int d = 2; d < n; d++)
+        if (L % d == 0) off += d;
+    return off;
+}
+__host__ __device__ constexpr int tw_full_size(int L) { return 4 * tw_table_size(L); }
 
 template <bool WARP> __device__ __forceinline__ void stage_barrier() {
     if constexpr (WARP) __syncwarp(); else __syncthreads();
@@ -238,7 +250,24 @@ __device__ __forceinline__ void fft_run(cx<T> (&v)[E], SM sm, int q, const cx<T>
             const cx<T> *__restrict__ twn = tw + TWO;
             if constexpr (sizeof(T) == 4) {
                 cx<T> wp[R];
-                twiddle_powers<T, R>(wp, twn, k);
+                if constexpr (SPNS_F32_TW_POW) {
+                    constexpr int P2 = tw_pow_offset(L, Ns * R, 2), P4 = tw_pow_offset(L, Ns * R, 4),
+                                  P8 = tw_pow_offset(L, Ns * R, 8);
+                    wp[1] = twn[k];
+#pragma unroll
+                    for (int r = 2; r < R; r++) {
+                        if (r == 2) wp[r] = tw[P2 + k];
+                        else if (r == 4) wp[r] = tw[P4 + k];
+                        else if (r == 8) wp[r] = tw[P8 + k];
+                        else {
+                            int hb = 1;
+                            while (hb * 2 <= r) hb *= 2;
+                            wp[r] = cmul(wp[hb], wp[r - hb]);
+                        }
+                    }
+                } else {
+                    twiddle_powers<T, R>(wp, twn, k);
+                }
 #pragma unroll
                 for (int r = 1; r < R; r++) v[m * R + r] = INV ? cmulc(v[m * R + r], wp[r]) : cmul(v[m * R + r], wp[r]);
             } else {

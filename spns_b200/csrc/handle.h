@@ -312,10 +312,11 @@ int spns_fail(spns_handle *h, int code, const char *fmt, ...);
 
 // Twiddle table w_L^m = exp(-2 pi i m / L), computed in extended precision, followed
 // by the per-stage sub-tables w_n^m = w_L^{m L/n} (copies of base entries) for every
-// divisor n < L of L, in increasing n (spns::tw_sub_offset); allocated in stream
+// divisor n < L of L, in increasing n (spns::tw_sub_offset), and the power tables
+// w_n^{r k} for r = 2, 4, 8 (spns::tw_pow_offset); allocated in stream
 // order on `st` (no device-wide synchronisation).
 template <typename T> inline void *spns_make_twiddles(int L, cudaStream_t st) {
-    const int total = spns::tw_table_size(L);
+    const int total = spns::tw_full_size(L);
     std::vector<spns::cx<T>> t(total);
     for (int m = 0; m < L; m++) {
         long double ang = 2.0L * 3.14159265358979323846264338327950288L * (long double)m / (long double)L;
@@ -327,6 +328,12 @@ template <typename T> inline void *spns_make_twiddles(int L, cudaStream_t st) {
         const int off = spns::tw_sub_offset(L, n);
         for (int m = 0; m < n; m++) t[off + m] = t[(long long)m * (L / n)];
     }
+    for (int r = 2; r <= 8; r *= 2)
+        for (int n = 2; n <= L; n++) {
+            if (L % n) continue;
+            const int off = spns::tw_pow_offset(L, n, r);
+            for (int k = 0; k < n; k++) t[off + k] = t[(long long)((r * k) % n) * (L / n)];
+        }
     void *d = nullptr;
     if (cudaMallocAsync(&d, sizeof(spns::cx<T>) * total, st) != cudaSuccess) return nullptr;
     if (cudaMemcpyAsync(d, t.data(), sizeof(spns::cx<T>) * total, cudaMemcpyHostToDevice, st) != cudaSuccess ||
