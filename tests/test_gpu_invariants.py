@@ -76,3 +76,22 @@ def test_eddy_viscosity_stats_match_the_oracle(N):
     assert np.max(np.abs(g - r) / r) < 1e-11, (g, r)
     dns = HIT(make_args(N, nu=3.283e-4), k41_ranks=4)
     assert np.all(dns.eddy_viscosity_stats() == 0.0)
+
+
+@pytest.mark.parametrize("box", [(512, 32, 32), (32, 512, 32), (32, 32, 512)], ids=["x768", "y768", "z768"])
+def test_invariant_spectra_at_length_768(box):
+    """The invariant passes (nine gradients through the inverse x and y passes, the
+    invariants in the z pass, five forward transforms) are their own instantiations per
+    FFT length: each axis in turn at the N=512 length, from a field with energy in every
+    retained mode."""
+    import oracle as O
+    from gpu_util import broadband_field
+    from spns_b200.hit import HIT
+    args = make_args(0, nu=3.283e-4, Ns=box)
+    U = broadband_field(*box, seed=5)
+    gpu = HIT(args, k41_ranks=-1)
+    ref = O.OracleHIT(args)
+    for h in (gpu, ref):
+        h.set_compact(U)
+    _close(gpu.Recalculate_Invariants_Distribution(), ref.Recalculate_Invariants_Distribution(), 1e-10)
+    gpu.close()
