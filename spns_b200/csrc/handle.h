@@ -132,7 +132,7 @@ template <typename T, int L, int ALT> using ShapeK2A = typename std::conditional
 template <typename T, int L, int ALT> using ShapeK5A = typename std::conditional<ALT != 0, ShapeT<T, L, SPNS_ALT_E, ShapeSel<T>::K5_T>, ShapeK5<T, L>>::type;
 
 // Rotational z pass with pair-by-pair bulk-copy staging, persistent
-// (k3_rot_staged, zpass_warp.cuh): used at lengths from SPNS_ZS_MIN_L up to 768.
+// (k3_rot_staged, zpass_staged.cuh): used at lengths from SPNS_ZS_MIN_L up to 768.
 // Per precision: E values per thread, PB pencils per block, SLOTS physical slots
 // in shared memory (of four), MINB resident blocks per SM for the register budget.
 #ifndef SPNS_ZS_MIN_L
@@ -148,10 +148,10 @@ template <typename T, int L, int ALT> using ShapeK5A = typename std::conditional
 #define SPNS_ZS_PB 2
 #endif
 #ifndef SPNS_ZS_SLOTS
-#define SPNS_ZS_SLOTS 0
-#endif
+#define SPNS_ZS_SLOTS 1           // double at 768: one slot in shared memory and 3 blocks per SM,
+#endif                            // 13.73 against 13.94 ms with all four in registers and 2 blocks
 #ifndef SPNS_ZS_MINB
-#define SPNS_ZS_MINB 2
+#define SPNS_ZS_MINB 3
 #endif
 #ifndef SPNS_F32_ZS_E
 #define SPNS_F32_ZS_E 12
