@@ -144,14 +144,17 @@ template <typename T, int L, int ALT> using ShapeK5A = typename std::conditional
 #ifndef SPNS_ZS_E
 #define SPNS_ZS_E 12
 #endif
+// Double at 768, N=512: one pencil per block, two of the four slots in shared memory and
+// 6 blocks per SM (12 warps) 12.97 ms; two pencils per block with one slot and 3 blocks
+// 13.74, with no slot and 2 blocks 13.94; one pencil with one slot 13.19 (6 blocks), 14.42 (7).
 #ifndef SPNS_ZS_PB
-#define SPNS_ZS_PB 2
+#define SPNS_ZS_PB 1
 #endif
 #ifndef SPNS_ZS_SLOTS
-#define SPNS_ZS_SLOTS 1           // double at 768: one slot in shared memory and 3 blocks per SM,
-#endif                            // 13.73 against 13.94 ms with all four in registers and 2 blocks
+#define SPNS_ZS_SLOTS 2
+#endif
 #ifndef SPNS_ZS_MINB
-#define SPNS_ZS_MINB 3
+#define SPNS_ZS_MINB 6
 #endif
 #ifndef SPNS_F32_ZS_E
 #define SPNS_F32_ZS_E 12
