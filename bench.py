@@ -40,7 +40,7 @@ SEED = 2024
 METRIC = "time steps/s, forced DNS N=512 (FFT 768^3), FP64"
 # kernels behind the per-pass event names at N=512, FP64 (the z pass at length 768 is the
 # persistent pair-staged kernel)
-KERNEL_SYMBOL = {"k3_z": "k3_rot_staged<double,768,E=12,2 pencils>", "k1_inv_x": "k1_inv_x<double,768,12,4>",
+KERNEL_SYMBOL = {"k3_z": "k3_rot_staged<double,768,E=12,1 pencil per block,2 slots in shared memory>", "k1_inv_x": "k1_inv_x<double,768,12,4>",
                  "k2_inv_y": "k2_inv_y<double,768,24,8>", "k4_fwd_y": "k4_fwd_y<double,768,24,8>",
                  "k5_fwd_x": "k5_fwd_x<double,768,24,4>", "k6_sweep": "k6_sweep<double,kappa>"}
 
